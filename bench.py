@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the polyspectrum estimator: bispectrum configurations per
+second on a 64-configuration theta sweep at 512^3.
+
+Workload (one "step"): an XHI_DENS field (dens*(1 - xHII)) of 512^3 float32
+cells in a 400 Mpc/h box - xHII from 32000 seeded ionised spheres, dens =
+1 + lognormal delta (P ~ k^-2) - phase-only, DERIVED binning, kbinwidth 1;
+four (k1, k2) sweeps {(0.2,0.5), (0.5,0.8), (0.8,1.2), (1.0,1.5)} h/Mpc of 16
+theta bins each = 64 bispectrum configurations with their polygon counts.
+A step runs the forward transform of the field and all 64 configurations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is device-timed with inputs resident
+in HBM; `e2e` is the same step through the C-ABI from pinned host inputs with
+the host->device copies and the result read-back inside the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bispectrum configs/s @512^3 batched-FP32 vs plain FP64-GPU, rel err<=1e-5"
+UNIT = "configs/s"
+PAIRS = [(0.2, 0.5), (0.5, 0.8), (0.8, 1.2), (1.0, 1.5)]
+
+
+def workload(grid: int):
+    return dict(workload=f"xhi_dens_{grid}^3_phase_derived_theta_sweep_64cfg", grid=grid, box=400.0,
+                spheres=int(round(32000 * (grid / 512) ** 3)), seed_ion=3, alpha=2.0, seed_dens=4,
+                pairs=PAIRS, num_values=16, binning="DERIVED", kbinwidth=1.0, use_only_phase=1)
+
+
+def make_inputs(w):
+    from polyspectrum_b200 import synth
+    dens, xhii = synth.xhi_dens_inputs(w["grid"], w["box"], w["spheres"], w["seed_ion"], w["alpha"],
+                                       w["seed_dens"])
+    return dens, xhii
+
+
+def make_cfgs(ps, w):
+    import ctypes as C
+    allc = []
+    for k1, k2 in w["pairs"]:
+        cfgs, _, _ = ps.read_params_to_kvectors(w["grid"], w["box"], 3, k1=k1, k2=k2,
+                                                num_values=w["num_values"],
+                                                kbinningCase=ps.PS_BIN_DERIVED)
+        allc += [cfgs[i] for i in range(len(cfgs))]
+    arr = (ps.ps_cfg * len(allc))()
+    for i, g in enumerate(allc):
+        C.memmove(C.byref(arr[i]), C.byref(g), C.sizeof(ps.ps_cfg))
+    return arr
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: str):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "50",
+                 "-i", index], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        rows = []
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(f[1]), smax=float(f[2]), power=float(f[3]),
+                                 hw=f[5], hwt=f[6], swt=f[7], swp=f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("swp", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(name)
+        return dict(sm_mhz=float(np.median([r["sm"] for r in rows])), sm_max_mhz=rows[0]["smax"],
+                    reasons=sorted(reasons), samples=len(rows),
+                    power_w_max=max(r["power"] for r in rows))
+
+
+def gpu_index(local_rank: int) -> str:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        parts = [p.strip() for p in vis.split(",") if p.strip()]
+        if local_rank < len(parts):
+            return parts[local_rank]
+    return str(local_rank)
+
+
+# --------------------------------------------------------------------------- CPU
+def cpu_reference_sample(w, dens, xhii, first: int = 0, count: int = 1):
+    """Time the reference's CPU implementation on `count` configurations of the
+    workload.  Uses oracle/_ref (the reference's own C, FFT shim) when built,
+    else the oracle restatement.  Returns (configs/s, kind, cores, sample, seconds)."""
+    import oracle
+    k1, k2 = w["pairs"][0]
+    p = oracle.RunParams(grid_size=w["grid"], box_size=w["box"], which_field=2,
+                         use_only_phase=w["use_only_phase"], n=3, equilateral=0, k1=k1, k2=k2,
+                         num_values=w["num_values"], kbinning=1, kbinwidth=w["kbinwidth"])
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("PS_SHIM_THREADS", str(cores))
+    t0 = time.time()
+    if oracle.ref_available():
+        r = oracle.ref_run(p, dens, xhii, first=first, count=count)
+        kind = "reference"
+        t_fwd, t_cfg = r.t_forward, r.t_configs
+    else:
+        t_a = time.time()
+        r = oracle.ora_run(p, dens, xhii, max_cfg=count)
+        kind = "port"
+        t_cfg = time.time() - t_a
+        t_fwd = 0.0
+    wall = time.time() - t0
+    per_cfg = t_cfg / max(count, 1) + t_fwd / 64.0
+    sample = (f"{count} of the 64 configurations (k1,k2)={w['pairs'][0]}, theta index {first}"
+              f"{'..' + str(first + count - 1) if count > 1 else ''}, at {w['grid']}^3 plus the forward "
+              f"transform amortised over 64; reference C + FFT shim (FFTW not installed), shim FFT on "
+              f"{cores} threads, estimator loops single-threaded as in the reference; "
+              f"t_forward={t_fwd:.2f}s t_configs={t_cfg:.2f}s")
+    return 1.0 / per_cfg, kind, cores, sample, wall
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU implementation (rank 0 only)."""
+    if rank != 0:
+        return
+    w = workload(args.grid)
+    dens, xhii = make_inputs(w)
+    # CPU work has no warm-up effects; one configuration per step (~20-40 s
+    # at 512^3), at most 3 timed steps so the run ends within a few minutes.
+    steps = max(1, min(args.steps, 3))
+    vals = []
+    info = None
+    t_all = time.time()
+    for s in range(steps):
+        v, kind, cores, sample, wall = cpu_reference_sample(w, dens, xhii, first=s, count=1)
+        vals.append(1.0 / v)
+        info = (kind, cores, sample)
+    per_cfg = float(np.mean(vals))
+    value = 1.0 / per_cfg
+    kind, cores, sample = info
+    out = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=steps,
+               warmup=0, requested_steps=args.steps, requested_warmup=args.warmup,
+               ms_per_step=per_cfg * 1e3, higher_is_better=True, scaling="weak",
+               vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
+               config=dict(workload=w["workload"], grid=w["grid"], box=w["box"],
+                           binning="DERIVED", use_only_phase=1, configs_per_sweep=64),
+               cpu_baseline=dict(value=value, unit=UNIT, cores=cores, kind=kind,
+                                 sample=f"per step: {sample}"),
+               e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+               wall_s=time.time() - t_all)
+    print(json.dumps(out), flush=True)
+
+
+# --------------------------------------------------------------------------- GPU
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import polyspectrum_b200 as ps
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = workload(args.grid)
+    dens_np, xhii_np = make_inputs(w)
+    N, box = w["grid"], w["box"]
+    cfgs = make_cfgs(ps, w)
+    ncfg = len(cfgs)
+
+    stream = torch.cuda.current_stream(dev)
+    ctx = ps.Context(N, box, methods=ps.PS_FP32_BATCHED, device=local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    dens = torch.from_numpy(dens_np).to(dev)
+    xhii = torch.from_numpy(xhii_np).to(dev)
+    launches = [0]
+
+    def step():
+        ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+        launches[0] += ctx.last_timing()[1]
+        out = ctx.batch(cfgs, ps.PS_FP32_BATCHED)
+        launches[0] += ctx.last_timing()[1]
+        return out
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(args.warmup, 3)):
+        res = step()
+    B32, N32 = res[0].copy(), res[1].copy()
+
+    # ---- timed region (inputs resident in HBM, larger than L2: no flush needed)
+    clocks = ClockSampler(gpu_index(local_rank))
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches[0] = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_step = ms / args.steps
+    value = world * ncfg / (ms_step / 1e3)
+    timed_launches = launches[0]
+
+    # ---- per-kernel roofline over a second pass of the same steps, events per launch
+    ctx.set_profiling(True)
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    stats = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    peak, peak_kind = measured_peak()
+    dom = max(stats, key=lambda s: s["ms"]) if stats else None
+    total_ms = sum(s["ms"] for s in stats) or 1.0
+    roof = None
+    if dom:
+        achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+                tr = json.load(f)
+            traffic = tr.get(dom["name"], {}).get("bytes_per_launch_512")
+        except Exception:
+            pass
+        roof = dict(bound="hbm", kernel=dom["name"], achieved=achieved, peak=peak,
+                    peak_source=peak_kind, unit="GB/s", frac=achieved / peak,
+                    traffic=traffic, alg_bytes_per_launch=dom["bytes"] / dom["launches"],
+                    avg_launch_ms=dom["ms"] / dom["launches"], launches=dom["launches"],
+                    share_of_kernel_time=dom["ms"] / total_ms)
+    all_alg = sum(s["bytes"] for s in stats)
+    kernels = {s["name"]: dict(launches=s["launches"] // args.steps,
+                               ms_per_step=s["ms"] / args.steps,
+                               GBps=(s["bytes"] / (s["ms"] / 1e3) / 1e9) if s["ms"] > 0 and s["bytes"] > 0 else None)
+               for s in stats}
+
+    # ---- end to end: pinned host inputs, copies and result read-back inside
+    dens_h = torch.from_numpy(dens_np).pin_memory()
+    xhii_h = torch.from_numpy(xhii_np).pin_memory()
+
+    def step_e2e():
+        ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens_h, xhii_h, use_only_phase=1)
+        return ctx.batch(cfgs, ps.PS_FP32_BATCHED)
+
+    step_e2e()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t0
+    ms_e2e = max_over_ranks(max(e0.elapsed_time(e1), t_wall * 1e3))
+    e2e_value = world * ncfg / (ms_e2e / args.steps / 1e3)
+    h2d = 2 * N ** 3 * 4
+    d2h = ncfg * 2 * 8 + 6 * 16  # B, Npoly per configuration + derived ranges of the leg shells
+
+    # ---- plain FP64 method on a sample of the same configurations (rank 0)
+    plain = None
+    if rank == 0 and not args.no_plain:
+        del ctx
+        torch.cuda.empty_cache()
+        sel = [0, 16, 32, 48] if ncfg >= 49 else list(range(min(4, ncfg)))
+        import ctypes as C
+        sub = (ps.ps_cfg * len(sel))()
+        for i, q in enumerate(sel):
+            C.memmove(C.byref(sub[i]), C.byref(cfgs[q]), C.sizeof(ps.ps_cfg))
+        with ps.Context(N, box, methods=ps.PS_FP64_PLAIN, device=local_rank) as c64:
+            c64.set_stream(stream.cuda_stream)
+            c64.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+            c64.batch(sub[:1], ps.PS_FP64_PLAIN)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            c64.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_fwd64 = e0.elapsed_time(e1)
+            e0.record(stream)
+            B64, N64, _, _ = c64.batch(sub, ps.PS_FP64_PLAIN)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_cfg64 = e0.elapsed_time(e1) / len(sel)
+        per_cfg64 = t_cfg64 + t_fwd64 / ncfg
+        b32 = B32[sel]
+        rel = np.abs(b32 - B64) / np.abs(B64)
+        plain = dict(configs_per_s=1e3 / per_cfg64, ms_per_config=t_cfg64, forward_ms=t_fwd64,
+                     sample=f"configurations {sel} of the sweep",
+                     batched_vs_plain_speedup=value / world / (1e3 / per_cfg64),
+                     max_rel_err_B_fp32_vs_fp64=float(rel.max()),
+                     counts_equal=bool(np.array_equal(N32[sel], np.rint(N64))))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, sample, wall = cpu_reference_sample(w, dens_np, xhii_np)
+        cpu = dict(value=v, unit=UNIT, cores=cores, kind=kind, sample=sample)
+
+    if rank == 0:
+        out = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
+                   warmup=max(args.warmup, 3), ms_per_step=ms_step, higher_is_better=True,
+                   scaling="weak", vs_baseline=None, dtype="f32 (FP64 counts and sums)",
+                   data="synthetic (seeded XHI_DENS field: 32000 spheres x lognormal density)",
+                   config=dict(workload=w["workload"], grid=N, box=box, pairs=w["pairs"],
+                               theta_bins=w["num_values"], configs_per_step=ncfg,
+                               binning="DERIVED", kbinwidth=1.0, use_only_phase=1,
+                               l2="inputs (2 x 512 MiB) and every pass larger than L2; no flush",
+                               parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+                   e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d,
+                            d2h_bytes_per_step=d2h, ms_per_step=ms_e2e / args.steps),
+                   gpu_launches=timed_launches, roofline=roof,
+                   whole_step=dict(alg_bytes=all_alg / args.steps,
+                                   achieved_GBps=all_alg / args.steps / (ms_step / 1e3) / 1e9),
+                   kernels=kernels, clocks=clk, plain_fp64=plain, cpu_baseline=cpu)
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=512, help="grid size (the workload is 512)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,183 @@
+/*
+ * ps_gpu.h - C-ABI of the B200 polyspectrum estimator (libpsgpu.so).
+ *
+ * Drop-in boundary for annehutter/polyspectrum's FFT estimator: the calls in
+ * src/run.c that
+ *   - build the transformed field     get_FT_field()            input_field.c:40  (run.c:47)
+ *   - normalise it to phases          calc_phase_3D_fftw_array() utils_fftw.c:78 (run.c:48-49)
+ *   - evaluate one configuration      polyspectrum()            polyspectrum.c:51 (run.c:87)
+ *   - count its polygons              num_polygons()            polyspectrum.c:163 (run.c:91)
+ *   - generate the k-configurations   read_params_to_kvectors() kvectors.c:46 + run.c:56-84
+ * are replaced by the entry points below.  Host code stays C; every argument
+ * is a plain pointer or scalar.  All functions return PS_OK (0) or a negative
+ * PS_ERR_* status and never exit the process.
+ *
+ * Conventions
+ *   - The context owns all device memory; host arrays stay owned by the caller
+ *     and are read/written before the call returns.
+ *   - One context per host thread; each context runs on its own CUDA stream.
+ *   - Grids are N^3, row-major [i][j][l] as in the reference (filter.c:59),
+ *     N a power of two in [16, 1024].
+ *   - Transforms follow FFTW's unnormalised convention (fft.c:17).
+ */
+#ifndef PS_GPU_H
+#define PS_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+#define PS_OK 0
+#define PS_ERR_ARG (-1)          /* invalid argument                          */
+#define PS_ERR_OOM (-2)          /* device or host allocation failed          */
+#define PS_ERR_IO (-3)           /* file could not be read (short read)       */
+#define PS_ERR_CUDA (-4)         /* CUDA runtime / kernel error               */
+#define PS_ERR_TIMEOUT (-5)      /* a bounded device wait expired             */
+#define PS_ERR_NONFINITE (-6)    /* non-finite input where finite is required */
+#define PS_ERR_UNSUPPORTED (-7)  /* valid for the reference, not implemented  */
+#define PS_ERR_UNDEFINED (-8)    /* the reference's behaviour is undefined    */
+
+/* ---- estimator methods ----------------------------------------------------- */
+/* PS_FP64_PLAIN: the reference dataflow in FP64, one configuration at a time:
+ *   per leg one inverse transform of F*dk and one of F (polyspectrum.c:72-133),
+ *   running products, grid sums, reference normalisation (polyspectrum.c:155).
+ * PS_FP32_BATCHED: all configurations of a call planned together: shells are
+ *   deduplicated, shared leg pairs are transformed once, closing legs of a
+ *   shared pair are folded by Parseval's identity into one k-space pass, field
+ *   transforms run in FP32 with FP64 accumulation, polygon counts are computed
+ *   in FP64 and rounded per mode, so they are exact integers. */
+#define PS_FP64_PLAIN 1
+#define PS_FP32_BATCHED 2
+
+/* ---- field selection (input_field.c:40-81, confObj whichField) ------------- */
+#define PS_FIELD_DENS 0     /* densityFile                                  */
+#define PS_FIELD_XHII 1     /* ionFile                                      */
+#define PS_FIELD_XHI_DENS 2 /* dens*(1 - xHII), input_field.c:22-37         */
+
+/* ---- kbinningCase (confObj.c:98-105) ---------------------------------------- */
+#define PS_BIN_DEFAULT 0
+#define PS_BIN_DERIVED 1
+#define PS_BIN_GIVEN 2
+#define PS_BIN_WATKINSON 3
+
+/* ---- where an input pointer lives ------------------------------------------ */
+#define PS_MEM_HOST 0
+#define PS_MEM_DEVICE 1
+
+#define PS_MAX_LEGS 8
+
+typedef struct ps_gpu_ctx ps_gpu_ctx;
+
+/* One configuration: the arguments of polyspectrum() (polyspectrum.h:7) minus
+ * the grid.  kmin/kmax are in/out exactly as there: DERIVED binning writes the
+ * derived ranges of every leg back (polyspectrum.c:83, :89-93). */
+typedef struct {
+    int n;                      /* number of legs, 2..PS_MAX_LEGS            */
+    int kbinningCase;           /* PS_BIN_*                                  */
+    double kbinwidth;           /* in units of the fundamental mode          */
+    double k[PS_MAX_LEGS];      /* leg lengths [h/Mpc]                       */
+    double kmin[PS_MAX_LEGS];   /* in/out                                    */
+    double kmax[PS_MAX_LEGS];   /* in/out                                    */
+} ps_cfg;
+
+/* Parameters of a run, the confObj keys that shape the configuration list
+ * (confObj.h:24-58). */
+typedef struct {
+    int grid_size;
+    double box_size;            /* as read from the ini file (double)        */
+    int n;
+    int equilateral;
+    double k1, k2;
+    int num_values;
+    double theta;
+    double kbinwidth;
+    int kbinningCase;
+    double dcosTheta;
+} ps_run_params;
+
+/* Create a context for an N^3 grid.  boxsize is the reference's grid box size
+ * (grid.h:9 stores it as float: pass (double)(float)L).  methods is a mask of
+ * PS_FP64_PLAIN | PS_FP32_BATCHED; the field spectra those methods need are
+ * computed by ps_gpu_set_field.  device < 0 keeps the current device. */
+int ps_gpu_create(ps_gpu_ctx **ctx, int nbins, double boxsize, int methods, int device);
+
+/* Load a field and run the forward transform (+ optional phase normalisation):
+ * replaces get_FT_field (input_field.c:40-81) and calc_phase_3D_fftw_array
+ * (utils_fftw.c:78-93, run.c:48-49).  which selects the field as whichField
+ * does; dens / xhii are N^3 float (is_double = 0) or double (is_double = 1)
+ * arrays in host (PS_MEM_HOST) or device (PS_MEM_DEVICE) memory; the one a
+ * field does not use may be NULL.  use_only_phase == 1 normalises every mode
+ * to unit modulus; a zero mode becomes NaN as in the reference. */
+int ps_gpu_set_field(ps_gpu_ctx *ctx, int which, const void *dens, const void *xhii,
+                     int is_double, int mem, int use_only_phase);
+
+/* ps_gpu_create + ps_gpu_set_field for a single field (DENS slot). */
+int ps_gpu_init(ps_gpu_ctx **ctx, int nbins, double boxsize, const void *field,
+                int field_is_double, int use_only_phase, int methods);
+
+/* One configuration with the context's first method: polyspectrum()
+ * (polyspectrum.c:51-161) and num_polygons() (polyspectrum.c:163-252) in one
+ * call.  B = V^(n-1) N^(-3n) Re sum prod D / Re sum prod I with V the cube of
+ * the context's box size; Npoly = Re sum prod I / N^3. */
+int ps_gpu_polyspectrum(ps_gpu_ctx *ctx, int n, const double *k, double *kmin, double *kmax,
+                        double kbinwidth, int kbinningCase, double *B, double *Npoly);
+
+/* nconf configurations with an explicit method (PS_FP64_PLAIN evaluates them
+ * one by one; PS_FP32_BATCHED plans them together).  kappa_or_NULL receives a
+ * condition number per configuration: sum |terms| / |sum terms| of the final
+ * FP64 sum the method evaluates (grid sum or Parseval k-space sum). */
+int ps_gpu_polyspectrum_batch(ps_gpu_ctx *ctx, int method, int nconf, ps_cfg *cfgs, double *B,
+                              double *Npoly, double *kappa_or_NULL);
+
+/* Gradient dB/d(delta) of one configuration with respect to the real input
+ * field (the array the forward transform read), written to out as N^3 float
+ * (out_is_double = 0) or double (1) in host or device memory (out_mem).  No
+ * reference counterpart; defined for use_only_phase = 0. */
+int ps_gpu_grad(ps_gpu_ctx *ctx, int method, int n, const double *k, const double *kmin,
+                const double *kmax, double kbinwidth, int kbinningCase, void *out,
+                int out_is_double, int out_mem);
+
+/* The configuration list of a run: read_params_to_kvectors (kvectors.c:46-147)
+ * plus the per-configuration kpolygon bookkeeping of run.c:56-84.  Writes at
+ * most max_cfg entries to cfgs (and the sweep values to k_out / theta_out,
+ * NaN where the run has no theta; either may be NULL) and returns the number
+ * of configurations, or a negative status (n < 2 or n > 3 are refused as
+ * kvectors.c:60-64, :140-144 refuse them). */
+int ps_make_configs(const ps_run_params *p, ps_cfg *cfgs, int max_cfg, double *k_out,
+                    double *theta_out);
+
+/* Use a caller-provided CUDA stream (cudaStream_t passed as void*); NULL
+ * returns to the context's own stream. */
+int ps_gpu_set_stream(ps_gpu_ctx *ctx, void *stream);
+
+/* Device timing of the last ps_gpu_* compute call on the context, in ms
+ * (CUDA events on the context's stream), and the number of kernels it launched. */
+int ps_gpu_last_timing(ps_gpu_ctx *ctx, double *ms, long long *kernel_launches);
+
+/* Per-kernel device timing.  When profiling is on, every kernel the context
+ * launches is bracketed by CUDA events on the context's stream and charged,
+ * with its algorithmic HBM bytes (the bytes its pass must read and write at
+ * minimum), to its kernel family.  ps_gpu_kernel_stats synchronises and
+ * returns up to max families; the counters reset when profiling is switched
+ * on.  No reference counterpart (the reference has only a total wall time,
+ * main.c:38-82). */
+typedef struct {
+    char name[32];        /* kernel family                                  */
+    long long launches;
+    double ms;            /* summed device time                             */
+    double bytes;         /* summed algorithmic bytes                       */
+} ps_kernel_stat;
+int ps_gpu_set_profiling(ps_gpu_ctx *ctx, int on);
+int ps_gpu_kernel_stats(ps_gpu_ctx *ctx, ps_kernel_stat *out, int max);
+
+void ps_gpu_finalize(ps_gpu_ctx *ctx);
+const char *ps_gpu_strerror(int status);
+/* Text of the last error on the calling thread (empty if none). */
+const char *ps_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PS_GPU_H */

@@ -31,12 +31,28 @@ _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 
 
+def reference_checkout() -> str | None:
+    """The reference checkout the Makefile's `ref` target compiles (its REF
+    variable, or $PS_REFERENCE_DIR), if it is present on this machine."""
+    path = os.environ.get("PS_REFERENCE_DIR")
+    if not path:
+        with open(os.path.join(HERE, "Makefile")) as f:
+            for line in f:
+                if line.startswith("REF ?="):
+                    path = line.split("?=", 1)[1].strip()
+                    break
+    return path if path and os.path.isdir(os.path.join(path, "src")) else None
+
+
 def build_oracle(ref: bool = False) -> None:
     """Build the restatement (and, when asked and the reference checkout is
     present, the reference harness)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        src = reference_checkout()
+        if src is None:
+            raise FileNotFoundError("reference checkout not present")
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}"], check=True)
 
 
 class _OraParams(C.Structure):

@@ -1,0 +1,1180 @@
+// libpsgpu: C-ABI, context, launch plumbing and the two estimator methods.
+#include <math.h>
+#include <stdarg.h>
+
+#include <cmath>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/ps_gpu.h"
+#include "ps_launch.cuh"
+
+namespace ps {
+PS_EXTERN_L3(float)
+PS_EXTERN_L3(double)
+}  // namespace ps
+
+using namespace ps;
+
+// =========================================================================
+// errors
+// =========================================================================
+namespace {
+thread_local char g_err[512] = {0};
+
+int fail(int code, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+}  // namespace
+
+#define PS_CK(x)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (x);                                                                \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(e_ == cudaErrorMemoryAllocation ? PS_ERR_OOM : PS_ERR_CUDA,          \
+                        "%s: %s (%s:%d)", #x, cudaGetErrorString(e_), __FILE__, __LINE__);  \
+    } while (0)
+#define PS_TRY(x)               \
+    do {                        \
+        int rc_ = (x);          \
+        if (rc_ != PS_OK) return rc_; \
+    } while (0)
+
+// =========================================================================
+// context
+// =========================================================================
+template <typename T> struct PrecBufs {
+    V2<T>* tw = nullptr;    // W_N^m, m in [0, N)
+    V2<T>* spec = nullptr;  // field spectrum, row stride S
+    V2<T>* work = nullptr;  // work spectrum (band-limited strides <= S)
+    T* ra = nullptr;        // real grids
+    T* rb = nullptr;
+    int S = 0;
+    bool have_spec = false;
+};
+
+struct ps_gpu_ctx {
+    int N = 0;
+    double L = 0.0;  // (double)(float) box size, grid.h:9
+    int methods = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    PrecBufs<float> f;
+    PrecBufs<double> d;
+    double* partials = nullptr;
+    size_t partials_cap = 0;
+    double* dsums = nullptr;  // device scalars
+    size_t dsums_cap = 0;
+    Shell* dshells = nullptr;
+    size_t dshells_cap = 0;
+    unsigned long long* dminmax = nullptr;
+    size_t dminmax_cap = 0;
+    void* stage[2] = {nullptr, nullptr};
+    size_t stage_bytes = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    long long launches = 0;
+    int use_only_phase = 0;
+    bool field_set = false;
+    // per-kernel profiling (ps_gpu_set_profiling)
+    struct ProfRec {
+        int kind;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    bool prof_on = false;
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    double prof_ms[16] = {0};
+    double prof_bytes[16] = {0};
+    long long prof_n[16] = {0};
+};
+
+namespace {
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+bool pow2_ok(int n) { return n >= 16 && n <= 1024 && (n & (n - 1)) == 0; }
+double ref_pi() { return acos(-1.0); }  // filter.c:19
+
+template <typename T> int alloc_dev(T** p, size_t count)
+{
+    if (*p) return PS_OK;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(PS_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", sizeof(T) * count,
+                    cudaGetErrorString(e));
+    }
+    return PS_OK;
+}
+
+template <typename T> int init_prec(ps_gpu_ctx* c, PrecBufs<T>& b)
+{
+    const int N = c->N;
+    b.S = round_up(N / 2 + 1, PencilWidth<T>::value);
+    const size_t nspec = (size_t)N * N * b.S;
+    const size_t nreal = (size_t)N * N * N;
+    PS_TRY(alloc_dev(&b.tw, N));
+    PS_TRY(alloc_dev(&b.spec, nspec));
+    PS_TRY(alloc_dev(&b.work, nspec));
+    PS_TRY(alloc_dev(&b.ra, nreal));
+    PS_TRY(alloc_dev(&b.rb, nreal));
+    std::vector<V2<T>> h(N);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int m = 0; m < N; m++) {
+        const long double a = two_pi * (long double)m / (long double)N;
+        h[m].x = (T)cosl(a);
+        h[m].y = (T)(-sinl(a));
+    }
+    PS_CK(cudaMemcpy(b.tw, h.data(), sizeof(V2<T>) * N, cudaMemcpyHostToDevice));
+    return PS_OK;
+}
+
+template <typename T> void free_prec(PrecBufs<T>& b)
+{
+    cudaFree(b.tw);
+    cudaFree(b.spec);
+    cudaFree(b.work);
+    cudaFree(b.ra);
+    cudaFree(b.rb);
+    b = PrecBufs<T>();
+}
+
+int ensure_partials(ps_gpu_ctx* c, size_t n)
+{
+    if (n <= c->partials_cap) return PS_OK;
+    cudaFree(c->partials);
+    c->partials = nullptr;
+    c->partials_cap = 0;
+    PS_TRY(alloc_dev(&c->partials, n));
+    c->partials_cap = n;
+    return PS_OK;
+}
+int ensure_sums(ps_gpu_ctx* c, size_t n)
+{
+    if (n <= c->dsums_cap) return PS_OK;
+    cudaFree(c->dsums);
+    c->dsums = nullptr;
+    c->dsums_cap = 0;
+    PS_TRY(alloc_dev(&c->dsums, n));
+    c->dsums_cap = n;
+    return PS_OK;
+}
+int ensure_shells(ps_gpu_ctx* c, size_t n)
+{
+    if (n <= c->dshells_cap) return PS_OK;
+    cudaFree(c->dshells);
+    c->dshells = nullptr;
+    c->dshells_cap = 0;
+    PS_TRY(alloc_dev(&c->dshells, n));
+    c->dshells_cap = n;
+    return PS_OK;
+}
+int ensure_minmax(ps_gpu_ctx* c, size_t n)
+{
+    if (n <= c->dminmax_cap) return PS_OK;
+    cudaFree(c->dminmax);
+    c->dminmax = nullptr;
+    c->dminmax_cap = 0;
+    PS_TRY(alloc_dev(&c->dminmax, n));
+    c->dminmax_cap = n;
+    return PS_OK;
+}
+
+// =========================================================================
+// launch plumbing (runtime N -> template N)
+// =========================================================================
+#define PS_SWITCH_N(N, BODY)                       \
+    switch (N) {                                   \
+    case 16: { constexpr int NN = 16; BODY; } break;   \
+    case 32: { constexpr int NN = 32; BODY; } break;   \
+    case 64: { constexpr int NN = 64; BODY; } break;   \
+    case 128: { constexpr int NN = 128; BODY; } break; \
+    case 256: { constexpr int NN = 256; BODY; } break; \
+    case 512: { constexpr int NN = 512; BODY; } break; \
+    case 1024: { constexpr int NN = 1024; BODY; } break; \
+    default: return fail(PS_ERR_UNSUPPORTED, "grid size %d not supported", N); \
+    }
+
+template <typename T> PrecBufs<T>& bufs(ps_gpu_ctx* c);
+template <> PrecBufs<float>& bufs<float>(ps_gpu_ctx* c) { return c->f; }
+template <> PrecBufs<double>& bufs<double>(ps_gpu_ctx* c) { return c->d; }
+
+}  // namespace
+
+int ps::launch_fail(cudaError_t e, const char* what)
+{
+    return fail(e == cudaErrorMemoryAllocation ? PS_ERR_OOM : PS_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+}
+
+namespace {
+
+// ---------------------------------------------------------------- profiling
+enum KernelFamily {
+    KF_FWD_Z = 0, KF_PASS_Y, KF_FWD_X_STORE, KF_FWD_X_DOT, KF_INV_X, KF_INV_Z, KF_SUM, KF_DERIVED,
+    KF_FINAL, KF_COUNT
+};
+const char* const kFamilyName[KF_COUNT] = {"fwd_z_r2c", "pass_y", "fwd_x_store", "fwd_x_dot",
+                                           "inv_x_masked", "inv_z_c2r", "sum_partials",
+                                           "derived_range", "finalize"};
+
+int prof_fold(ps_gpu_ctx* c)
+{
+    if (c->prof.empty()) return PS_OK;
+    PS_CK(cudaStreamSynchronize(c->stream));
+    for (const auto& r : c->prof) {
+        float ms = 0.f;
+        PS_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        c->prof_ms[r.kind] += ms;
+        c->prof_bytes[r.kind] += r.bytes;
+        c->prof_n[r.kind] += 1;
+    }
+    c->prof.clear();
+    c->ev_used = 0;
+    return PS_OK;
+}
+
+cudaEvent_t prof_event(ps_gpu_ctx* c)
+{
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+
+// Bracket one kernel launch: begin() before, end() after.
+struct Prof {
+    ps_gpu_ctx* c;
+    cudaEvent_t a = nullptr;
+    explicit Prof(ps_gpu_ctx* cc) : c(cc)
+    {
+        if (c->prof_on) {
+            if (c->prof.size() >= 4096) prof_fold(c);
+            a = prof_event(c);
+            if (a) cudaEventRecord(a, c->stream);
+        }
+    }
+    void end(int kind, double bytes)
+    {
+        c->launches++;
+        if (!a) return;
+        cudaEvent_t b = prof_event(c);
+        if (!b) return;
+        cudaEventRecord(b, c->stream);
+        c->prof.push_back({kind, a, b, bytes});
+    }
+};
+
+int sum_partials(ps_gpu_ctx* c, int nblocks, int ncols, double* out, int out_stride)
+{
+    Prof pf(c);
+    k_sum_partials<<<ncols, 1024, 0, c->stream>>>(c->partials, nblocks, out, out_stride);
+    pf.end(KF_SUM, 8.0 * nblocks * ncols);
+    return PS_OK;
+}
+
+// Inverse 3D transform of shell-filtered data, band-limited to the shell,
+// with the real-space epilogue.  mode: LOAD_MASKED (F * spectrum) or LOAD_UNIT (F).
+// For reducing epilogues the grid sum lands in *dsum (device).
+template <typename T>
+int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, const T* aux, int epi,
+              int power, double* dsum)
+{
+    PrecBufs<T>& B = bufs<T>(c);
+    const int N = c->N;
+    const int hb = std::min(band, N / 2) + 1;
+    const int S = round_up(hb, PencilWidth<T>::value);
+    const bool reduce = epi == EPI_MUL_REDUCE || epi == EPI_REDUCE;
+    if (reduce) PS_TRY(ensure_partials(c, (size_t)N * N));
+    int nb = 0;
+    const double V = sizeof(V2<T>), NN2 = (double)N * N;
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, B.work, S, mode, dshell, N / 2 + 1, B.tw))));
+        pf.end(KF_INV_X, NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, true, B.tw))));
+        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_z(c->stream, B.work, S, hb, out, aux, epi, power, c->partials, B.tw, &nb))));
+        const double real = NN2 * N * sizeof(T);
+        const double extra = (epi == EPI_STORE ? real : 0.0) + (epi == EPI_MUL_STORE ? 2.0 * real : 0.0) +
+                             (epi == EPI_MUL_REDUCE ? real : 0.0);
+        pf.end(KF_INV_Z, NN2 * hb * V + extra);
+    }
+    if (reduce) PS_TRY(sum_partials(c, nb, 1, dsum, 1));
+    PS_CK(cudaGetLastError());
+    return PS_OK;
+}
+
+// Forward transform of a real grid into B.work (row stride returned), rows
+// truncated to h < hout.
+template <typename T>
+int r2c_work(ps_gpu_ctx* c, int kind, const void* a, const void* b, int hout, int* stride_out)
+{
+    PrecBufs<T>& B = bufs<T>(c);
+    const int N = c->N;
+    const int S = round_up(hout, PencilWidth<T>::value);
+    const double V = sizeof(V2<T>), NN2 = (double)N * N;
+    const double src_bytes = kind == SRC_T ? sizeof(T) : (kind == SRC_F32 ? 4.0 : kind == SRC_F64 ? 8.0 : kind == SRC_XHI_F32 ? 8.0 : 16.0);
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.work, S, hout, B.tw))));
+        pf.end(KF_FWD_Z, NN2 * N * src_bytes + NN2 * hout * V);
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, false, B.tw))));
+        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
+    }
+    *stride_out = S;
+    return PS_OK;
+}
+
+// Forward field transform into B.spec (+ phase normalisation).
+template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, const void* b)
+{
+    PrecBufs<T>& B = bufs<T>(c);
+    const int N = c->N;
+    const int epi = c->use_only_phase == 1 ? SPEC_STORE_PHASE : SPEC_STORE;
+    const double V = sizeof(V2<T>), NN2 = (double)N * N, H = N / 2 + 1;
+    const double src_bytes = kind == SRC_F32 ? 4.0 : kind == SRC_F64 ? 8.0 : kind == SRC_XHI_F32 ? 8.0 : 16.0;
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, N / 2 + 1, B.tw))));
+        pf.end(KF_FWD_Z, NN2 * N * src_bytes + NN2 * H * V);
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tw))));
+        pf.end(KF_PASS_Y, 2.0 * NN2 * B.S * V);
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.spec, B.S, N / 2 + 1, epi, B.spec, B.S, nullptr, 0,
+                                                nullptr, 0, nullptr, B.tw, nullptr))));
+        pf.end(KF_FWD_X_STORE, 2.0 * NN2 * H * V);
+    }
+    PS_CK(cudaGetLastError());
+    B.have_spec = true;
+    return PS_OK;
+}
+
+// Dot / count pass over a forward-transformed work buffer (stride S, band
+// hvalid) for up to MAX_DOT_SHELLS shells per launch; results to dout[0..ns).
+template <typename T>
+int dot_pass(ps_gpu_ctx* c, int epi, int S, int hvalid, const Shell* dshells, int ns, double* dout)
+{
+    PrecBufs<T>& B = bufs<T>(c);
+    const int N = c->N;
+    for (int s0 = 0; s0 < ns; s0 += MAX_DOT_SHELLS) {
+        const int cnt = std::min(MAX_DOT_SHELLS, ns - s0);
+        const size_t blocks = (size_t)N * (S / PencilWidth<T>::value);
+        PS_TRY(ensure_partials(c, blocks * MAX_DOT_SHELLS));
+        int nb = 0;
+        {
+            Prof pf(c);
+            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.work, S, hvalid, epi, nullptr, 0, B.spec, B.S,
+                                                    dshells + s0, cnt, c->partials, B.tw, &nb))));
+            pf.end(KF_FWD_X_DOT, (double)N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
+        }
+        PS_TRY(sum_partials(c, nb, cnt, dout + s0, 1));
+    }
+    PS_CK(cudaGetLastError());
+    return PS_OK;
+}
+
+// =========================================================================
+// shells
+// =========================================================================
+struct ShellKey {
+    int kind;
+    double a, b, half;
+    bool operator<(const ShellKey& o) const
+    {
+        return std::tie(kind, a, b, half) < std::tie(o.kind, o.a, o.b, o.half);
+    }
+};
+
+int band_of(double r, int N)
+{
+    if (!(r >= 0.0) || !std::isfinite(r) || r >= (double)(N / 2)) return N / 2;
+    return std::min(N / 2, (int)floor(r) + 2);
+}
+
+Shell make_shell(int kind, double k, double kmin, double kmax, double binwidth, double L, int N)
+{
+    const double pi = ref_pi();
+    Shell s;
+    memset(&s, 0, sizeof(s));
+    s.kind = kind;
+    s.half = 0.5 * binwidth;
+    volatile double big = 1.e30;
+    s.min2_init = big * big;
+    s.kk = k / (2. * pi) * L;           // filter.c:36
+    s.mmin = kmin / (2. * pi) * L;      // filter.c:137
+    s.mmax = kmax / (2. * pi) * L;      // filter.c:138
+    const double ah = fabs(s.half);
+    double rb;
+    switch (kind) {
+    case SHELL_DEFAULT: rb = s.kk + ah; break;
+    case SHELL_RANGE: rb = s.mmax + ah; break;
+    case SHELL_WATKINSON: rb = s.kk + 1.7320508075688772 * ah + 1e-9; break;
+    default: rb = std::max(s.mmin, s.mmax) + 1.7320508075688772 * ah + 1e-9; break;
+    }
+    s.band = band_of(rb, N);
+    return s;
+}
+
+// DERIVED ranges (filter.c:78-114) of DEFAULT shells, computed on the device.
+int derive_ranges(ps_gpu_ctx* c, const std::vector<Shell>& sh, std::vector<double>& kmin,
+                  std::vector<double>& kmax)
+{
+    const int ns = (int)sh.size();
+    kmin.assign(ns, 0.0);
+    kmax.assign(ns, 0.0);
+    if (!ns) return PS_OK;
+    PS_TRY(ensure_shells(c, ns));
+    PS_TRY(ensure_minmax(c, 2 * (size_t)ns));
+    PS_CK(cudaMemcpyAsync(c->dshells, sh.data(), sizeof(Shell) * ns, cudaMemcpyHostToDevice, c->stream));
+    std::vector<unsigned long long> init(2 * ns);
+    for (int s = 0; s < ns; s++) {
+        double m2 = sh[s].min2_init, z = 0.0;
+        memcpy(&init[2 * s], &m2, 8);
+        memcpy(&init[2 * s + 1], &z, 8);
+    }
+    PS_CK(cudaMemcpyAsync(c->dminmax, init.data(), 16 * (size_t)ns, cudaMemcpyHostToDevice, c->stream));
+    const int N = c->N;
+    for (int s = 0; s < ns; s++) {
+        const int band = std::min(sh[s].band, N / 2);
+        const int hmax = band;
+        const long long total = (long long)(2 * band + 1) * (2 * band + 1) * (hmax + 1);
+        const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+        Prof pf(c);
+        k_derived_range<<<blocks, 256, 0, c->stream>>>(N, c->dshells + s, hmax, c->dminmax + 2 * s);
+        pf.end(KF_DERIVED, 0.0);
+    }
+    PS_CK(cudaGetLastError());
+    PS_CK(cudaMemcpyAsync(init.data(), c->dminmax, 16 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
+    PS_CK(cudaStreamSynchronize(c->stream));
+    const double pi = ref_pi();
+    for (int s = 0; s < ns; s++) {
+        double m2, x2;
+        memcpy(&m2, &init[2 * s], 8);
+        memcpy(&x2, &init[2 * s + 1], 8);
+        const double rmin = sqrt(m2), rmax = sqrt(x2);
+        kmin[s] = rmin * 2. * pi / c->L;  // filter.c:112-113
+        kmax[s] = rmax * 2. * pi / c->L;
+    }
+    return PS_OK;
+}
+
+// calc_k3_min_and_max (filter.c:291-319), same operation order.
+void closing_leg_range(const double* k, double* kmin, double* kmax)
+{
+    const double cth = (k[0] * k[0] + k[1] * k[1] - k[2] * k[2]) / (2. * k[0] * k[1]);
+    const double a[8] = {kmin[0], kmin[0], kmax[0], kmax[0], k[0], kmax[0], k[0], kmin[0]};
+    const double b[8] = {kmin[1], kmax[1], kmin[1], kmax[1], kmax[1], k[1], kmin[1], k[1]};
+    double lo = 1.e30, hi = 0.;
+    for (int q = 0; q < 8; q++) {
+        const double t = a[q] * a[q] + b[q] * b[q] - 2. * a[q] * b[q] * cth;
+        if (t < lo) lo = t;
+        if (t > hi) hi = t;
+    }
+    kmin[2] = sqrt(lo);
+    kmax[2] = sqrt(hi);
+}
+
+// Resolve every leg of every configuration to a shell (polyspectrum.c:79-118),
+// running the DERIVED reductions on the device and writing the derived ranges
+// back into the configurations.
+int resolve_legs(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, std::vector<std::vector<Shell>>& legs)
+{
+    const int N = c->N;
+    const double L = c->L;
+    legs.assign(nconf, {});
+    // pass 1: DEFAULT shells whose DERIVED range is needed
+    std::map<ShellKey, int> dkey;
+    std::vector<Shell> dsh;
+    for (int q = 0; q < nconf; q++) {
+        const ps_cfg& g = cfgs[q];
+        if (g.n < 2 || g.n > PS_MAX_LEGS) return fail(PS_ERR_ARG, "config %d: n=%d out of range", q, g.n);
+        if (g.kbinningCase == PS_BIN_DERIVED) {
+            if (g.n != 3)
+                return fail(PS_ERR_UNDEFINED,
+                            "config %d: DERIVED binning with n=%d is undefined in the reference "
+                            "(calc_kn_min_and_max, filter.c:321-325)", q, g.n);
+            for (int l = 0; l < g.n - 1; l++) {
+                ShellKey key{SHELL_DEFAULT, g.k[l], 0.0, 0.5 * g.kbinwidth};
+                if (!dkey.count(key)) {
+                    dkey[key] = (int)dsh.size();
+                    dsh.push_back(make_shell(SHELL_DEFAULT, g.k[l], 0, 0, g.kbinwidth, L, N));
+                }
+            }
+        }
+    }
+    std::vector<double> dmin, dmax;
+    PS_TRY(derive_ranges(c, dsh, dmin, dmax));
+    // pass 2: every leg
+    for (int q = 0; q < nconf; q++) {
+        ps_cfg& g = cfgs[q];
+        const int n = g.n;
+        auto& ls = legs[q];
+        for (int l = 0; l < n; l++) {
+            const bool last = l == n - 1;
+            switch (g.kbinningCase) {
+            case PS_BIN_DERIVED:
+                if (!last) {
+                    const int id = dkey[ShellKey{SHELL_DEFAULT, g.k[l], 0.0, 0.5 * g.kbinwidth}];
+                    g.kmin[l] = dmin[id];
+                    g.kmax[l] = dmax[id];
+                    ls.push_back(dsh[id]);
+                } else {
+                    closing_leg_range(g.k, g.kmin, g.kmax);
+                    ls.push_back(make_shell(SHELL_RANGE, 0, g.kmin[l], g.kmax[l], g.kbinwidth, L, N));
+                }
+                break;
+            case PS_BIN_GIVEN:
+                ls.push_back(last ? make_shell(SHELL_RANGE, 0, g.kmin[l], g.kmax[l], g.kbinwidth, L, N)
+                                  : make_shell(SHELL_DEFAULT, g.k[l], 0, 0, g.kbinwidth, L, N));
+                break;
+            case PS_BIN_WATKINSON:
+                ls.push_back(last ? make_shell(SHELL_WATKINSON_RANGE, 0, g.kmin[l], g.kmax[l],
+                                               g.kbinwidth, L, N)
+                                  : make_shell(SHELL_WATKINSON, g.k[l], 0, 0, g.kbinwidth, L, N));
+                break;
+            default:
+                ls.push_back(make_shell(SHELL_DEFAULT, g.k[l], 0, 0, g.kbinwidth, L, N));
+                break;
+            }
+        }
+    }
+    return PS_OK;
+}
+
+bool same_shell(const Shell& a, const Shell& b) { return memcmp(&a, &b, sizeof(Shell)) == 0; }
+
+// =========================================================================
+// finalisation: B = pow(V,n-1)*pow(N,-3n)*sumD/sumI (polyspectrum.c:155)
+// =========================================================================
+__global__ void k_finalize(int nconf, const double* __restrict__ coef, const double* __restrict__ sumD,
+                           const double* __restrict__ sumI, double inv_n3, int count_mode,
+                           double* __restrict__ out)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nconf) return;
+    const double sD = sumD[q];
+    double sI, np;
+    if (count_mode) {  // sumI holds the exact polygon count
+        np = sumI[q];
+        sI = __dmul_rn(np, 1.0 / inv_n3);
+    } else {
+        sI = sumI[q];
+        np = __dmul_rn(sI, inv_n3);
+    }
+    out[2 * q] = __ddiv_rn(__dmul_rn(coef[q], sD), sI);
+    out[2 * q + 1] = count_mode ? np : __ddiv_rn(sI, 1.0 / inv_n3);
+}
+
+double norm_coef(double L, int N, int n)
+{
+    const double volume = L * L * L;
+    return pow(volume, n - 1) * pow(N, -n * 3);
+}
+
+// =========================================================================
+// method 1: plain FP64, reference dataflow
+// =========================================================================
+int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
+{
+    if (!c->d.have_spec) return fail(PS_ERR_ARG, "FP64 spectrum not available (methods mask)");
+    std::vector<std::vector<Shell>> legs;
+    const int N = c->N;
+    PS_TRY(ensure_sums(c, 4 * (size_t)nconf + 8));
+    PS_TRY(ensure_shells(c, PS_MAX_LEGS));
+    std::vector<double> coef(nconf);
+    for (int q = 0; q < nconf; q++) {
+        PS_TRY(resolve_legs(c, 1, cfgs + q, legs));
+        const int n = cfgs[q].n;
+        PS_CK(cudaMemcpyAsync(c->dshells, legs[0].data(), sizeof(Shell) * n, cudaMemcpyHostToDevice,
+                              c->stream));
+        double* sD = c->dsums + q;
+        double* sI = c->dsums + nconf + q;
+        for (int pass = 0; pass < 2; pass++) {  // 0: D = IFFT[F dk], 1: I = IFFT[F]
+            const int mode = pass == 0 ? LOAD_MASKED : LOAD_UNIT;
+            double* prod = pass == 0 ? c->d.ra : c->d.rb;
+            for (int l = 0; l < n; l++) {
+                const int epi = l == 0 ? EPI_STORE : (l < n - 1 ? EPI_MUL_STORE : EPI_MUL_REDUCE);
+                PS_TRY(c2r_shell<double>(c, mode, c->dshells + l, legs[0][l].band, prod, prod, epi, 1,
+                                         pass == 0 ? sD : sI));
+            }
+        }
+        coef[q] = norm_coef(c->L, N, n);
+        // the host shell table is rewritten by the next config: keep order
+        PS_CK(cudaStreamSynchronize(c->stream));
+    }
+    double* dcoef = c->dsums + 2 * nconf;
+    PS_CK(cudaMemcpyAsync(dcoef, coef.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice, c->stream));
+    double* dout = nullptr;
+    PS_TRY(alloc_dev(&dout, 2 * (size_t)nconf));
+    const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
+    {
+        Prof pf(c);
+        k_finalize<<<(nconf + 127) / 128, 128, 0, c->stream>>>(nconf, dcoef, c->dsums, c->dsums + nconf,
+                                                               inv_n3, 0, dout);
+        pf.end(KF_FINAL, 0.0);
+    }
+    std::vector<double> h(2 * nconf);
+    cudaError_t e1 = cudaMemcpyAsync(h.data(), dout, sizeof(double) * 2 * nconf, cudaMemcpyDeviceToHost,
+                                     c->stream);
+    cudaError_t e2 = cudaStreamSynchronize(c->stream);
+    cudaFree(dout);
+    PS_CK(e1);
+    PS_CK(e2);
+    for (int q = 0; q < nconf; q++) {
+        B[q] = h[2 * q];
+        Np[q] = h[2 * q + 1];
+    }
+    return PS_OK;
+}
+
+// =========================================================================
+// method 2: batched FP32 (FP64 counts)
+// =========================================================================
+struct Group {  // n=3 configurations sharing the leg pair (a, b)
+    int a, b;
+    std::vector<int> cfg;    // configuration indices
+    std::vector<int> third;  // shell id of each configuration's remaining leg
+};
+
+int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
+{
+    if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available (methods mask)");
+    const int N = c->N;
+    std::vector<std::vector<Shell>> legs;
+    PS_TRY(resolve_legs(c, nconf, cfgs, legs));
+    // unique shells
+    std::vector<Shell> uniq;
+    std::vector<std::vector<int>> lid(nconf);
+    for (int q = 0; q < nconf; q++) {
+        for (const Shell& s : legs[q]) {
+            int id = -1;
+            for (size_t u = 0; u < uniq.size(); u++)
+                if (same_shell(uniq[u], s)) { id = (int)u; break; }
+            if (id < 0) { id = (int)uniq.size(); uniq.push_back(s); }
+            lid[q].push_back(id);
+        }
+    }
+    // device shell table: unique shells, then per-group third-leg lists
+    std::vector<Group> groups;
+    std::vector<int> direct;      // configurations evaluated leg by leg
+    std::vector<int> pairs2;      // n == 2 configurations (Parseval, no transform)
+    {
+        std::map<std::pair<int, int>, int> freq;
+        for (int q = 0; q < nconf; q++)
+            if (cfgs[q].n == 3) {
+                const auto& v = lid[q];
+                for (int x = 0; x < 3; x++)
+                    for (int y = x + 1; y < 3; y++) freq[{std::min(v[x], v[y]), std::max(v[x], v[y])}]++;
+            }
+        std::map<std::pair<int, int>, int> gidx;
+        for (int q = 0; q < nconf; q++) {
+            const int n = cfgs[q].n;
+            if (n == 2) { pairs2.push_back(q); continue; }
+            if (n != 3) { direct.push_back(q); continue; }
+            const auto& v = lid[q];
+            int best = -1, bx = 0, by = 1;
+            for (int x = 0; x < 3; x++)
+                for (int y = x + 1; y < 3; y++) {
+                    const int f = freq[{std::min(v[x], v[y]), std::max(v[x], v[y])}];
+                    if (f > best) { best = f; bx = x; by = y; }
+                }
+            const int z = 3 - bx - by;
+            if (best < 2) { direct.push_back(q); continue; }
+            std::pair<int, int> key{std::min(v[bx], v[by]), std::max(v[bx], v[by])};
+            auto it = gidx.find(key);
+            if (it == gidx.end()) {
+                gidx[key] = (int)groups.size();
+                groups.push_back(Group{key.first, key.second, {}, {}});
+                it = gidx.find(key);
+            }
+            groups[it->second].cfg.push_back(q);
+            groups[it->second].third.push_back(v[z]);
+        }
+    }
+    // shell table layout: [uniq][group thirds...][pairs2: (a,b) interleaved? no: we pass a,b]
+    std::vector<Shell> table = uniq;
+    std::vector<int> gofs(groups.size());
+    for (size_t g = 0; g < groups.size(); g++) {
+        gofs[g] = (int)table.size();
+        for (int s : groups[g].third) table.push_back(uniq[s]);
+    }
+    PS_TRY(ensure_shells(c, table.size()));
+    PS_CK(cudaMemcpyAsync(c->dshells, table.data(), sizeof(Shell) * table.size(),
+                          cudaMemcpyHostToDevice, c->stream));
+    PS_TRY(ensure_sums(c, 4 * (size_t)nconf + 8));
+    double* sumD = c->dsums;
+    double* sumI = c->dsums + nconf;  // exact counts (count mode)
+    std::vector<double> coef(nconf);
+    for (int q = 0; q < nconf; q++) coef[q] = norm_coef(c->L, N, cfgs[q].n);
+
+    // ---- shared-pair groups: Parseval over the closing legs
+    for (size_t g = 0; g < groups.size(); g++) {
+        const Group& G = groups[g];
+        const Shell& sa = uniq[G.a];
+        const Shell& sb = uniq[G.b];
+        int hmax = 0;
+        for (int s : G.third) hmax = std::max(hmax, std::min(uniq[s].band, N / 2));
+        const int hout = hmax + 1;
+        const int ng = (int)G.cfg.size();
+        // scratch sums for the group, then scatter
+        double* gD = c->dsums + 2 * nconf;
+        double* gI = c->dsums + 3 * nconf;
+        // D part (FP32): P = D_a * D_b, transform, dot with dk over each closing shell
+        if (G.a == G.b) {
+            PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + G.a, sa.band, c->f.rb, nullptr, EPI_STORE, 2,
+                                    nullptr));
+        } else {
+            PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + G.a, sa.band, c->f.ra, nullptr, EPI_STORE, 1,
+                                    nullptr));
+            PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + G.b, sb.band, c->f.rb, c->f.ra,
+                                    EPI_MUL_STORE, 1, nullptr));
+        }
+        int S = 0;
+        PS_TRY(r2c_work<float>(c, SRC_T, c->f.rb, nullptr, hout, &S));
+        PS_TRY(dot_pass<float>(c, SPEC_DOT, S, hout, c->dshells + gofs[g], ng, gD));
+        // I part (FP64): counts
+        if (G.a == G.b) {
+            PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.rb, nullptr, EPI_STORE, 2,
+                                     nullptr));
+        } else {
+            PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.ra, nullptr, EPI_STORE, 1,
+                                     nullptr));
+            PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + G.b, sb.band, c->d.rb, c->d.ra,
+                                     EPI_MUL_STORE, 1, nullptr));
+        }
+        PS_TRY(r2c_work<double>(c, SRC_T, c->d.rb, nullptr, hout, &S));
+        PS_TRY(dot_pass<double>(c, SPEC_COUNT, S, hout, c->dshells + gofs[g], ng, gI));
+        for (int x = 0; x < ng; x++) {
+            PS_CK(cudaMemcpyAsync(sumD + G.cfg[x], gD + x, 8, cudaMemcpyDeviceToDevice, c->stream));
+            PS_CK(cudaMemcpyAsync(sumI + G.cfg[x], gI + x, 8, cudaMemcpyDeviceToDevice, c->stream));
+        }
+    }
+
+    // ---- n = 2: sum_x D_a D_b = N^3 sum_m F_a F_b |dk|^2 -> reuse the leg-by-leg path
+    for (int q : pairs2) direct.push_back(q);
+
+    // ---- leg by leg (singletons, n = 2, n > 3): running products with powers
+    for (int q : direct) {
+        const auto& v = lid[q];
+        std::vector<std::pair<int, int>> up;  // (shell, multiplicity)
+        for (int s : v) {
+            bool found = false;
+            for (auto& pr : up)
+                if (pr.first == s) { pr.second++; found = true; }
+            if (!found) up.push_back({s, 1});
+        }
+        const int r = (int)up.size();
+        for (int pass = 0; pass < 2; pass++) {
+            for (int x = 0; x < r; x++) {
+                int epi;
+                if (r == 1) epi = EPI_REDUCE;
+                else epi = x == 0 ? EPI_STORE : (x < r - 1 ? EPI_MUL_STORE : EPI_MUL_REDUCE);
+                const Shell& s = uniq[up[x].first];
+                if (pass == 0)
+                    PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + up[x].first, s.band, c->f.ra,
+                                            c->f.ra, epi, up[x].second, sumD + q));
+                else
+                    PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + up[x].first, s.band, c->d.ra,
+                                             c->d.ra, epi, up[x].second, sumI + q));
+            }
+        }
+    }
+    // direct configurations hold grid sums in sumI: convert them to counts
+    // (round(sumI / N^3), exact since the FP64 error is far below 1/2)
+    std::vector<double> hsD(nconf), hsI(nconf);
+    PS_CK(cudaMemcpyAsync(hsD.data(), sumD, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream));
+    PS_CK(cudaMemcpyAsync(hsI.data(), sumI, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream));
+    PS_CK(cudaStreamSynchronize(c->stream));
+    const double n3 = (double)N * (double)N * (double)N;
+    for (int q : direct) hsI[q] = nearbyint(hsI[q] / n3);
+    PS_CK(cudaMemcpyAsync(sumI, hsI.data(), 8 * (size_t)nconf, cudaMemcpyHostToDevice, c->stream));
+    double* dcoef = c->dsums + 2 * nconf;
+    PS_CK(cudaMemcpyAsync(dcoef, coef.data(), 8 * (size_t)nconf, cudaMemcpyHostToDevice, c->stream));
+    double* dout = nullptr;
+    PS_TRY(alloc_dev(&dout, 2 * (size_t)nconf));
+    {
+        Prof pf(c);
+        k_finalize<<<(nconf + 127) / 128, 128, 0, c->stream>>>(nconf, dcoef, sumD, sumI, 1.0 / n3, 1, dout);
+        pf.end(KF_FINAL, 0.0);
+    }
+    std::vector<double> h(2 * nconf);
+    cudaError_t e1 = cudaMemcpyAsync(h.data(), dout, 16 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e2 = cudaStreamSynchronize(c->stream);
+    cudaFree(dout);
+    PS_CK(e1);
+    PS_CK(e2);
+    for (int q = 0; q < nconf; q++) {
+        B[q] = h[2 * q];
+        Np[q] = h[2 * q + 1];
+    }
+    return PS_OK;
+}
+
+int timed_begin(ps_gpu_ctx* c)
+{
+    c->launches = 0;
+    PS_CK(cudaEventRecord(c->ev0, c->stream));
+    return PS_OK;
+}
+int timed_end(ps_gpu_ctx* c)
+{
+    PS_CK(cudaEventRecord(c->ev1, c->stream));
+    PS_CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    PS_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
+    return PS_OK;
+}
+
+}  // namespace
+
+// =========================================================================
+// C-ABI
+// =========================================================================
+extern "C" {
+
+const char* ps_gpu_strerror(int s)
+{
+    switch (s) {
+    case PS_OK: return "ok";
+    case PS_ERR_ARG: return "invalid argument";
+    case PS_ERR_OOM: return "out of memory";
+    case PS_ERR_IO: return "i/o error";
+    case PS_ERR_CUDA: return "CUDA error";
+    case PS_ERR_TIMEOUT: return "device wait timed out";
+    case PS_ERR_NONFINITE: return "non-finite input";
+    case PS_ERR_UNSUPPORTED: return "unsupported";
+    case PS_ERR_UNDEFINED: return "undefined in the reference";
+    default: return "unknown status";
+    }
+}
+
+const char* ps_gpu_last_error(void) { return g_err; }
+
+int ps_gpu_create(ps_gpu_ctx** out, int nbins, double boxsize, int methods, int device)
+{
+    g_err[0] = 0;
+    if (!out) return fail(PS_ERR_ARG, "ctx pointer is NULL");
+    *out = nullptr;
+    if (!pow2_ok(nbins)) return fail(PS_ERR_UNSUPPORTED, "grid size %d: need a power of two in [16,1024]", nbins);
+    if (!(boxsize > 0.0) || !std::isfinite(boxsize)) return fail(PS_ERR_ARG, "box size must be positive");
+    if (!(methods & (PS_FP64_PLAIN | PS_FP32_BATCHED)) || (methods & ~(PS_FP64_PLAIN | PS_FP32_BATCHED)))
+        return fail(PS_ERR_ARG, "methods mask %d invalid", methods);
+    int ndev = 0;
+    PS_CK(cudaGetDeviceCount(&ndev));
+    if (device >= ndev) return fail(PS_ERR_ARG, "device %d of %d", device, ndev);
+    if (device >= 0) PS_CK(cudaSetDevice(device));
+    ps_gpu_ctx* c = new ps_gpu_ctx();
+    c->N = nbins;
+    c->L = boxsize;
+    c->methods = methods;
+    cudaGetDevice(&c->device);
+    int rc = PS_OK;
+    do {
+        if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "stream creation failed");
+            break;
+        }
+        c->stream = c->own_stream;
+        if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "event creation failed");
+            break;
+        }
+        // the batched method transforms shells in FP32 and counts in FP64
+        if (methods & PS_FP32_BATCHED) {
+            if ((rc = init_prec(c, c->f)) != PS_OK) break;
+            if ((rc = init_prec(c, c->d)) != PS_OK) break;
+        }
+        if ((methods & PS_FP64_PLAIN) && (rc = init_prec(c, c->d)) != PS_OK) break;
+    } while (0);
+    if (rc != PS_OK) {
+        ps_gpu_finalize(c);
+        return rc;
+    }
+    *out = c;
+    return PS_OK;
+}
+
+int ps_gpu_set_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int is_double,
+                     int mem, int use_only_phase)
+{
+    g_err[0] = 0;
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    if (which < PS_FIELD_DENS || which > PS_FIELD_XHI_DENS) return fail(PS_ERR_ARG, "which=%d", which);
+    if (mem != PS_MEM_HOST && mem != PS_MEM_DEVICE) return fail(PS_ERR_ARG, "mem=%d", mem);
+    const void* a = which == PS_FIELD_XHII ? xhii : dens;
+    const void* b = which == PS_FIELD_XHI_DENS ? xhii : nullptr;
+    if (!a || (which == PS_FIELD_XHI_DENS && !b)) return fail(PS_ERR_ARG, "field pointer is NULL");
+    PS_CK(cudaSetDevice(c->device));
+    const size_t n3 = (size_t)c->N * c->N * c->N;
+    const size_t bytes = n3 * (is_double ? 8 : 4);
+    PS_TRY(timed_begin(c));
+    if (mem == PS_MEM_HOST) {
+        if (c->stage_bytes < bytes) {
+            cudaFree(c->stage[0]);
+            cudaFree(c->stage[1]);
+            c->stage[0] = c->stage[1] = nullptr;
+            c->stage_bytes = 0;
+            PS_TRY(alloc_dev((unsigned char**)&c->stage[0], bytes));
+            PS_TRY(alloc_dev((unsigned char**)&c->stage[1], bytes));
+            c->stage_bytes = bytes;
+        }
+        PS_CK(cudaMemcpyAsync(c->stage[0], a, bytes, cudaMemcpyHostToDevice, c->stream));
+        if (b) PS_CK(cudaMemcpyAsync(c->stage[1], b, bytes, cudaMemcpyHostToDevice, c->stream));
+        a = c->stage[0];
+        if (b) b = c->stage[1];
+    }
+    const int kind = b ? (is_double ? SRC_XHI_F64 : SRC_XHI_F32) : (is_double ? SRC_F64 : SRC_F32);
+    c->use_only_phase = use_only_phase;
+    c->f.have_spec = c->d.have_spec = false;
+    if (c->methods & PS_FP32_BATCHED) PS_TRY(forward_field<float>(c, kind, a, b));
+    if (c->methods & PS_FP64_PLAIN) PS_TRY(forward_field<double>(c, kind, a, b));
+    PS_TRY(timed_end(c));
+    c->field_set = true;
+    return PS_OK;
+}
+
+int ps_gpu_init(ps_gpu_ctx** ctx, int nbins, double boxsize, const void* field, int field_is_double,
+                int use_only_phase, int methods)
+{
+    PS_TRY(ps_gpu_create(ctx, nbins, boxsize, methods, -1));
+    int rc = ps_gpu_set_field(*ctx, PS_FIELD_DENS, field, nullptr, field_is_double, PS_MEM_HOST,
+                              use_only_phase);
+    if (rc != PS_OK) {
+        ps_gpu_finalize(*ctx);
+        *ctx = nullptr;
+    }
+    return rc;
+}
+
+int ps_gpu_polyspectrum_batch(ps_gpu_ctx* c, int method, int nconf, ps_cfg* cfgs, double* B,
+                              double* Npoly, double* kappa)
+{
+    g_err[0] = 0;
+    if (!c || !cfgs || !B || !Npoly || nconf < 0) return fail(PS_ERR_ARG, "NULL argument");
+    if (!c->field_set) return fail(PS_ERR_ARG, "no field loaded (ps_gpu_set_field)");
+    if (nconf == 0) return PS_OK;
+    if (method != PS_FP64_PLAIN && method != PS_FP32_BATCHED) return fail(PS_ERR_ARG, "method %d", method);
+    if (!(c->methods & method)) return fail(PS_ERR_ARG, "method %d not enabled for this context", method);
+    PS_CK(cudaSetDevice(c->device));
+    PS_TRY(timed_begin(c));
+    int rc = method == PS_FP64_PLAIN ? plain_batch(c, nconf, cfgs, B, Npoly)
+                                     : batched(c, nconf, cfgs, B, Npoly);
+    if (rc != PS_OK) return rc;
+    if (kappa)
+        for (int q = 0; q < nconf; q++) kappa[q] = NAN;
+    return timed_end(c);
+}
+
+int ps_gpu_polyspectrum(ps_gpu_ctx* c, int n, const double* k, double* kmin, double* kmax,
+                        double kbinwidth, int kbinningCase, double* B, double* Npoly)
+{
+    g_err[0] = 0;
+    if (!c || !k || !kmin || !kmax || !B || !Npoly) return fail(PS_ERR_ARG, "NULL argument");
+    if (n < 2 || n > PS_MAX_LEGS) return fail(PS_ERR_ARG, "n=%d out of range", n);
+    ps_cfg g;
+    memset(&g, 0, sizeof(g));
+    g.n = n;
+    g.kbinningCase = kbinningCase;
+    g.kbinwidth = kbinwidth;
+    for (int l = 0; l < n; l++) {
+        g.k[l] = k[l];
+        g.kmin[l] = kmin[l];
+        g.kmax[l] = kmax[l];
+    }
+    const int method = (c->methods & PS_FP64_PLAIN) ? PS_FP64_PLAIN : PS_FP32_BATCHED;
+    PS_TRY(ps_gpu_polyspectrum_batch(c, method, 1, &g, B, Npoly, nullptr));
+    for (int l = 0; l < n; l++) {
+        kmin[l] = g.kmin[l];
+        kmax[l] = g.kmax[l];
+    }
+    return PS_OK;
+}
+
+int ps_gpu_grad(ps_gpu_ctx* c, int method, int n, const double* k, const double* kmin,
+                const double* kmax, double kbinwidth, int kbinningCase, void* out, int out_is_double,
+                int out_mem)
+{
+    (void)c; (void)method; (void)n; (void)k; (void)kmin; (void)kmax; (void)kbinwidth;
+    (void)kbinningCase; (void)out; (void)out_is_double; (void)out_mem;
+    return fail(PS_ERR_UNSUPPORTED, "ps_gpu_grad: not built yet");
+}
+
+int ps_make_configs(const ps_run_params* p, ps_cfg* cfgs, int max_cfg, double* k_out, double* theta_out)
+{
+    g_err[0] = 0;
+    if (!p) return fail(PS_ERR_ARG, "params NULL");
+    const double pi = ref_pi();
+    const int n = p->n;
+    if (n < 2) return fail(PS_ERR_ARG, "n must be >= 2 (kvectors.c:60-64)");
+    if (n > 3) return fail(PS_ERR_UNSUPPORTED, "n > 3 not implemented in the reference (kvectors.c:140-144)");
+    int nval;
+    std::vector<double> kl, th;
+    double kpoly[3] = {0, 0, 0}, kpmin[3] = {0, 0, 0}, kpmax[3] = {0, 0, 0};
+    if (n == 2) {  // kvectors.c:75-96
+        if (p->num_values > 1) {
+            nval = p->grid_size / 2;
+            kl.resize(std::max(nval, 2));
+            for (int i = 0; i < nval; i++) kl[i] = 2. * pi / p->box_size * (double)(i + 1);
+        } else {
+            nval = 1;
+            kl = {p->k1, p->k1};  // kvectors.c:88-89
+        }
+        for (int i = 0; i < 2; i++) kpoly[i] = kpmin[i] = kpmax[i] = kl[i];
+    } else {  // kvectors.c:100-137
+        kpoly[0] = p->k1;
+        kpoly[1] = p->k2;
+        if (p->equilateral == 1) {
+            if (p->num_values <= 0) return fail(PS_ERR_ARG, "numValues must be > 0 (kvectors.c:107)");
+            nval = p->num_values;
+            kl.resize(nval);
+            const double kL = 2. * pi / p->box_size;
+            for (int i = 0; i < nval; i++) kl[i] = kL * pow(p->grid_size / 2, (double)(i + 1) / (double)nval);
+            th = {pi / 3.};
+        } else if (p->num_values > 1) {
+            nval = p->num_values;
+            kl.resize(nval);
+            th.resize(nval);
+            for (int i = 0; i < nval; i++) {
+                th[i] = pi * (double)i / (double)nval;
+                kl[i] = sqrt(p->k1 * p->k1 + p->k2 * p->k2 - 2. * p->k1 * p->k2 * cos(th[i]));
+            }
+        } else {
+            nval = 1;
+            th = {p->theta};
+            kl = {sqrt(p->k1 * p->k1 + p->k2 * p->k2 - 2. * p->k1 * p->k2 * cos(p->theta))};
+        }
+    }
+    for (int i = 0; i < nval && i < max_cfg; i++) {  // run.c:56-84
+        kpoly[n - 1] = kl[i];
+        if (n == 2) kpoly[0] = kl[i];
+        if (n == 3) {
+            const int ti = p->equilateral == 1 ? 0 : i;
+            if (p->equilateral == 1)
+                for (int j = 0; j < n; j++) kpoly[j] = kl[i];
+            if (p->kbinningCase >= 2) {  // calc_k3min / calc_k3max, kvectors.c:233-246
+                const double cmin = fmin(1., cos(th[ti]) + 0.5 * p->dcosTheta);
+                const double cmax = fmax(-1., cos(th[ti]) - 0.5 * p->dcosTheta);
+                kpmin[n - 1] = sqrt(kpoly[0] * kpoly[0] + kpoly[1] * kpoly[1] - 2. * kpoly[0] * kpoly[1] * cmin);
+                kpmax[n - 1] = sqrt(kpoly[0] * kpoly[0] + kpoly[1] * kpoly[1] - 2. * kpoly[0] * kpoly[1] * cmax);
+            }
+        }
+        if (cfgs) {
+            ps_cfg& g = cfgs[i];
+            memset(&g, 0, sizeof(g));
+            g.n = n;
+            g.kbinningCase = p->kbinningCase;
+            g.kbinwidth = p->kbinwidth;
+            for (int j = 0; j < n; j++) {
+                g.k[j] = kpoly[j];
+                g.kmin[j] = kpmin[j];
+                g.kmax[j] = kpmax[j];
+            }
+        }
+        if (k_out) k_out[i] = kl[i];
+        if (theta_out) theta_out[i] = th.empty() ? NAN : (p->equilateral == 1 ? th[0] : th[i]);
+    }
+    return nval;
+}
+
+int ps_gpu_set_stream(ps_gpu_ctx* c, void* stream)
+{
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return PS_OK;
+}
+
+int ps_gpu_last_timing(ps_gpu_ctx* c, double* ms, long long* launches)
+{
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    if (ms) *ms = c->last_ms;
+    if (launches) *launches = c->launches;
+    return PS_OK;
+}
+
+int ps_gpu_set_profiling(ps_gpu_ctx* c, int on)
+{
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    PS_TRY(prof_fold(c));
+    if (on && !c->prof_on) {
+        for (int q = 0; q < 16; q++) {
+            c->prof_ms[q] = c->prof_bytes[q] = 0.0;
+            c->prof_n[q] = 0;
+        }
+    }
+    c->prof_on = on != 0;
+    return PS_OK;
+}
+
+int ps_gpu_kernel_stats(ps_gpu_ctx* c, ps_kernel_stat* out, int max)
+{
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    PS_CK(cudaSetDevice(c->device));
+    PS_TRY(prof_fold(c));
+    int cnt = 0;
+    for (int q = 0; q < KF_COUNT; q++) {
+        if (!c->prof_n[q]) continue;
+        if (out && cnt < max) {
+            memset(&out[cnt], 0, sizeof(ps_kernel_stat));
+            snprintf(out[cnt].name, sizeof(out[cnt].name), "%s", kFamilyName[q]);
+            out[cnt].launches = c->prof_n[q];
+            out[cnt].ms = c->prof_ms[q];
+            out[cnt].bytes = c->prof_bytes[q];
+        }
+        cnt++;
+    }
+    return cnt;
+}
+
+void ps_gpu_finalize(ps_gpu_ctx* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_prec(c->f);
+    free_prec(c->d);
+    cudaFree(c->partials);
+    cudaFree(c->dsums);
+    cudaFree(c->dshells);
+    cudaFree(c->dminmax);
+    cudaFree(c->stage[0]);
+    cudaFree(c->stage[1]);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,129 @@
+// Common device types for the polyspectrum B200 kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ps {
+
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+template <typename T> using V2 = typename Vec2<T>::type;
+
+template <typename V> __device__ __forceinline__ V cadd(V a, V b) { return V{a.x + b.x, a.y + b.y}; }
+template <typename V> __device__ __forceinline__ V csub(V a, V b) { return V{a.x - b.x, a.y - b.y}; }
+template <typename V> __device__ __forceinline__ V cmul(V a, V b)
+{
+    return V{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename V> __device__ __forceinline__ V cconj(V a) { return V{a.x, -a.y}; }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, typename V> __device__ __forceinline__ V mul_mi(V a)
+{
+    if constexpr (INV) return V{-a.y, a.x};
+    else return V{a.y, -a.x};
+}
+template <typename V> __device__ __forceinline__ V czero() { return V{0, 0}; }
+
+// ---------------------------------------------------------------------------
+// Shell (k-space filter) descriptors.  The predicates restate the reference's
+// filter functions (src/filter.c) with the same FP64 operation order; the
+// intrinsics (__dadd_rn etc.) keep nvcc from contracting into FMA, so every
+// filter bit equals the one the reference's -std=c99 build computes.
+// ---------------------------------------------------------------------------
+enum ShellKind : int {
+    SHELL_DEFAULT = 0,         // construct_kfilter             filter.c:34-63
+    SHELL_RANGE = 1,           // construct_kfilter_with_kbinwidth filter.c:130-162
+    SHELL_WATKINSON = 2,       // construct_kfilter_Watkinson   filter.c:178-208
+    SHELL_WATKINSON_RANGE = 3  // construct_kfilter_Watkinson_kn filter.c:219-250
+};
+
+struct Shell {
+    int kind;
+    int band;      // every selected mode has |m_x|,|m_y|,|m_z| <= band (host bound)
+    double kk;     // k/(2 pi)*L           (DEFAULT, WATKINSON)
+    double mmin;   // kmin/(2 pi)*L        (RANGE kinds)
+    double mmax;   // kmax/(2 pi)*L        (RANGE kinds)
+    double half;   // 0.5*kbinwidth
+    double min2_init;  // 1e30*1e30, the squared start value of get_corners (filter.c:201,267)
+};
+
+// Lattice frequency of FFT index idx (filter.c:44-55).
+__device__ __forceinline__ int lattice_freq(int idx, int n) { return idx < (n >> 1) ? idx : idx - n; }
+
+// get_corners (filter.c:257-289) on squared radii: min/max over the 8 corners
+// of the cube of half-width e around m, folded into (min2, max2).
+__device__ __forceinline__ void corners_fold(int mx, int my, int mz, double e, double& min2,
+                                             double& max2)
+{
+    const double x = (double)mx, y = (double)my, z = (double)mz;
+    const double xm = __dmul_rn(__dsub_rn(x, e), __dsub_rn(x, e));
+    const double xp = __dmul_rn(__dadd_rn(x, e), __dadd_rn(x, e));
+    const double ym = __dmul_rn(__dsub_rn(y, e), __dsub_rn(y, e));
+    const double yp = __dmul_rn(__dadd_rn(y, e), __dadd_rn(y, e));
+    const double zm = __dmul_rn(__dsub_rn(z, e), __dsub_rn(z, e));
+    const double zp = __dmul_rn(__dadd_rn(z, e), __dadd_rn(z, e));
+    const double c[8] = {__dadd_rn(__dadd_rn(xm, ym), zm), __dadd_rn(__dadd_rn(xp, ym), zm),
+                         __dadd_rn(__dadd_rn(xm, yp), zm), __dadd_rn(__dadd_rn(xm, ym), zp),
+                         __dadd_rn(__dadd_rn(xp, yp), zm), __dadd_rn(__dadd_rn(xp, ym), zp),
+                         __dadd_rn(__dadd_rn(xm, yp), zp), __dadd_rn(__dadd_rn(xp, yp), zp)};
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        if (c[q] > max2) max2 = c[q];
+        if (c[q] < min2) min2 = c[q];
+    }
+}
+
+__device__ __forceinline__ bool shell_bit(const Shell& s, int mx, int my, int mz)
+{
+    switch (s.kind) {
+    case SHELL_DEFAULT: {
+        const double m = __dsqrt_rn((double)(mx * mx + my * my + mz * mz));
+        return fabs(__dsub_rn(s.kk, m)) <= s.half;
+    }
+    case SHELL_RANGE: {
+        const double m = __dsqrt_rn((double)(mx * mx + my * my + mz * mz));
+        return __dsub_rn(s.mmin, m) <= s.half && __dsub_rn(m, s.mmax) <= s.half;
+    }
+    case SHELL_WATKINSON: {
+        double min2 = s.min2_init, max2 = 0.0;
+        corners_fold(mx, my, mz, s.half, min2, max2);
+        const double pmin = __dsqrt_rn(min2), pmax = __dsqrt_rn(max2);
+        return pmin <= s.kk && s.kk <= pmax;
+    }
+    case SHELL_WATKINSON_RANGE: {
+        double min2 = s.min2_init, max2 = 0.0;
+        corners_fold(mx, my, mz, s.half, min2, max2);
+        const double pmin = __dsqrt_rn(min2), pmax = __dsqrt_rn(max2);
+        return (pmax >= s.mmax && pmin <= s.mmax) || (pmax <= s.mmax && pmin >= s.mmin) ||
+               (pmax >= s.mmin && pmin <= s.mmin);
+    }
+    default:
+        return false;
+    }
+}
+
+// Cheap necessary condition: outside the band cube nothing is selected.
+__device__ __forceinline__ bool in_band(const Shell& s, int mx, int my, int mz)
+{
+    return abs(mx) <= s.band && abs(my) <= s.band && abs(mz) <= s.band;
+}
+
+// Bitmask of the shells (of ns <= 32) that select mode m; one out-of-line
+// instance so the callers' unrolled loops stay small.
+static __device__ __noinline__ unsigned shell_bits(const Shell* __restrict__ sh, int ns, int mx, int my, int mz)
+{
+    unsigned bits = 0u;
+    for (int c = 0; c < ns; c++) {
+        const Shell s = sh[c];
+        if (in_band(s, mx, my, mz) && shell_bit(s, mx, my, mz)) bits |= 1u << c;
+    }
+    return bits;
+}
+
+// Half-spectrum weight: modes with 0 < h < N/2 stand for themselves and their
+// Hermitian mirrors.
+__device__ __forceinline__ int herm_weight(int h, int n) { return (h == 0 || h == (n >> 1)) ? 1 : 2; }
+
+}  // namespace ps

@@ -1,0 +1,6 @@
+// Explicit instantiation of the double pass kernels and their launchers.
+#include "ps_launch.cuh"
+
+namespace ps {
+PS_INSTANTIATE_L3(double)
+}  // namespace ps

@@ -1,0 +1,147 @@
+"""GPU parity: the CUDA library through its C-ABI against the CPU oracle on
+the same seeded inputs, for every binning case, n = 2 and 3, equilateral and
+theta sweeps, phase-only on and off, and the three field kinds.
+
+Tolerances (written here, checked per configuration):
+  * PS_FP64_PLAIN  : |dB| <= 1e-9 |B| + 1e-11 max|B| of the sweep;
+                     |dNpoly| <= 1e-7 max(1, Npoly)
+  * PS_FP32_BATCHED: |dB| <= 1e-5 |B| + 1e-6 max|B| of the sweep
+                     (the second term covers configurations whose sum cancels
+                     to near zero, where a relative error has no meaning);
+                     Npoly == round(Npoly_reference) exactly
+  * DERIVED k ranges written back: bit-identical for both methods.
+Configurations without any polygon (Npoly rounds to 0) have B = 0/0 in exact
+arithmetic; the reference returns a ratio of rounding residues there, the
+batched method NaN, so B is not compared for them.
+"""
+import numpy as np
+import pytest
+
+from _cases import field_args, fields, sweep_params
+
+pytestmark = pytest.mark.gpu
+
+TOL = {1: (1e-9, 1e-11), 2: (1e-5, 1e-6)}
+
+
+def run_both(ps, ora, n_grid, box, case, method):
+    dens, xhii = fields(n_grid, box)
+    dd, xx = field_args(case["which_field"], dens, xhii)
+    p = ora.RunParams(grid_size=n_grid, box_size=box, **case)
+    ref = ora.ora_run(p, dd, xx)
+    with ps.Context(n_grid, box, methods=method) as ctx:
+        ctx.get_FT_field(case["which_field"], dd, xx, use_only_phase=case["use_only_phase"])
+        got = ps.run_sweep(ctx, n_grid, box, case["n"], method=method,
+                           equilateral=case["equilateral"], k1=case["k1"], k2=case["k2"],
+                           num_values=case["num_values"], theta=case["theta"],
+                           kbinwidth=case["kbinwidth"], kbinningCase=case["kbinning"],
+                           dcosTheta=case["dcos_theta"])
+    return ref, got
+
+
+def check(ref, got, method, label=""):
+    rt, at = TOL[method]
+    np.testing.assert_array_equal(got.k, ref.k)
+    scale = np.nanmax(np.abs(ref.B)) if np.isfinite(ref.B).any() else 0.0
+    has = np.rint(ref.npoly) != 0
+    err = np.abs(got.B - ref.B)
+    bound = rt * np.abs(ref.B) + at * scale
+    bad = has & ~(err <= bound)
+    assert not bad.any(), f"{label} B mismatch: got {got.B[bad]} ref {ref.B[bad]}"
+    if method == 2:
+        np.testing.assert_array_equal(got.npoly, np.rint(ref.npoly), err_msg=label)
+    else:
+        assert np.all(np.abs(got.npoly - ref.npoly) <= 1e-7 * np.maximum(1, np.abs(ref.npoly))), label
+        np.testing.assert_array_equal(np.rint(got.npoly), np.rint(ref.npoly), err_msg=label)
+
+
+CASES = sweep_params(32, 200.0)
+
+
+@pytest.mark.parametrize("method", [1, 2], ids=["plain64", "batched32"])
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "n{n}_eq{equilateral}_kb{kbinning}_ph{use_only_phase}_f{which_field}".format(**c))
+def test_sweep_matches_oracle(gpu_lib, ora, case, method):
+    ref, got = run_both(gpu_lib, ora, 32, 200.0, case, method)
+    check(ref, got, method, str(case))
+    if case["kbinning"] == 1:
+        np.testing.assert_array_equal(got.kmin, ref.kmin)
+        np.testing.assert_array_equal(got.kmax, ref.kmax)
+
+
+@pytest.mark.parametrize("n_grid", [16, 64])
+@pytest.mark.parametrize("method", [1, 2], ids=["plain64", "batched32"])
+def test_other_grid_sizes(gpu_lib, ora, n_grid, method):
+    box = 150.0
+    kf = 2 * np.pi / box
+    case = dict(n=3, equilateral=0, k1=2.7 * kf, k2=4.1 * kf, num_values=5, theta=0.0,
+                kbinwidth=1.0, kbinning=1, dcos_theta=0.2, use_only_phase=0, which_field=2)
+    ref, got = run_both(gpu_lib, ora, n_grid, box, case, method)
+    check(ref, got, method)
+    np.testing.assert_array_equal(got.kmin, ref.kmin)
+
+
+@pytest.mark.parametrize("bw", [0.5, 2.0, 3.0])
+@pytest.mark.parametrize("kb", [0, 1, 2, 3])
+def test_binwidths(gpu_lib, ora, bw, kb):
+    box = 100.0
+    kf = 2 * np.pi / box
+    case = dict(n=3, equilateral=0, k1=3.0 * kf, k2=5.0 * kf, num_values=4, theta=0.0,
+                kbinwidth=bw, kbinning=kb, dcos_theta=0.15, use_only_phase=0, which_field=0)
+    for method in (1, 2):
+        ref, got = run_both(gpu_lib, ora, 32, box, case, method)
+        check(ref, got, method, f"bw={bw} kb={kb} m={method}")
+
+
+def test_single_config_api(gpu_lib, ora):
+    """ps_gpu_polyspectrum (one configuration, reference argument order)."""
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    dens, _ = fields(n_grid, box)
+    L = float(np.float32(box))
+    dk = ora.ora_forward(n_grid, 0, dens)
+    kf = 2 * np.pi / box
+    k = np.array([3.3 * kf, 4.2 * kf, 5.9 * kf])
+    for kb in (0, 1, 2, 3):
+        lo = np.array([0.0, 0.0, 5.0 * kf])
+        hi = np.array([0.0, 0.0, 6.5 * kf])
+        b_ref, _, _, lo_ref, hi_ref = ora.ora_polyspectrum(n_grid, dk, k, lo, hi, 1.0, kb, L)
+        n_ref = ora.ora_num_polygons(n_grid, k, lo_ref, hi_ref, 1.0, kb, L)
+        with ps.Context(n_grid, box, methods=ps.PS_FP64_PLAIN) as ctx:
+            ctx.get_FT_field(0, dens)
+            b, npol, lo2, hi2 = ctx.polyspectrum(3, k, lo, hi, 1.0, kb)
+        assert abs(b - b_ref) <= 1e-9 * abs(b_ref)
+        assert abs(npol - n_ref) <= 1e-7 * max(1.0, n_ref)
+        np.testing.assert_array_equal(lo2, lo_ref)
+        np.testing.assert_array_equal(hi2, hi_ref)
+
+
+def test_derived_n2_is_refused(gpu_lib):
+    ps = gpu_lib
+    with ps.Context(16, 100.0) as ctx:
+        ctx.get_FT_field(0, fields(16, 100.0)[0])
+        cfg = ps.make_cfg(2, [0.2, 0.2], [0.2, 0.2], [0.2, 0.2], 1.0, ps.PS_BIN_DERIVED)
+        for method in (1, 2):
+            with pytest.raises(ps.PsError) as e:
+                ctx.batch([cfg], method)
+            assert e.value.status == -8
+
+
+def test_device_resident_field(gpu_lib, ora):
+    """Field pointers in device memory (torch tensors) give the same result."""
+    import torch
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    dens, xhii = fields(n_grid, box)
+    dd, xx = field_args(2, dens, xhii)
+    cfgs, k, th = ps.read_params_to_kvectors(n_grid, box, 3, k1=0.1, k2=0.13, num_values=4,
+                                             kbinningCase=1)
+    outs = []
+    for mem in ("host", "device"):
+        with ps.Context(n_grid, box) as ctx:
+            if mem == "host":
+                ctx.get_FT_field(2, dd, xx)
+            else:
+                ctx.get_FT_field(2, torch.from_numpy(dd).cuda(), torch.from_numpy(xx).cuda())
+            outs.append(ctx.batch(cfgs, ps.PS_FP32_BATCHED)[:2])
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
