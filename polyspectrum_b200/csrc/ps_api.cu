@@ -859,6 +859,13 @@ int timed_end(ps_gpu_ctx* c)
 
 }  // namespace
 
+int ps::report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+Shell ps::host_shell(int kind, double k, double kmin, double kmax, double binwidth, double L, int N)
+{
+    return make_shell(kind, k, kmin, kmax, binwidth, L, N);
+}
+double ps::host_norm_coef(double L, int N, int n) { return norm_coef(L, N, n); }
+
 // =========================================================================
 // C-ABI
 // =========================================================================

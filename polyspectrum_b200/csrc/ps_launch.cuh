@@ -11,6 +11,12 @@
 namespace ps {
 
 int launch_fail(cudaError_t e, const char* what);
+// Records a message for ps_gpu_last_error() and returns code.
+int report_error(int code, const char* msg);
+// Shell descriptor as the context builds it (filter.c expressions, host side).
+Shell host_shell(int kind, double k, double kmin, double kmax, double binwidth, double L, int N);
+// pow(V, n-1) * pow(N, -3n) with V = L^3 (polyspectrum.c:155).
+double host_norm_coef(double L, int N, int n);
 
 #define PS_LTRY(x)                \
     do {                          \
