@@ -51,13 +51,30 @@ int fail(int code, const char* fmt, ...)
         if (rc_ != PS_OK) return rc_; \
     } while (0)
 
+#define PS_SWITCH_N(N, BODY)                       \
+    switch (N) {                                   \
+    case 16: { constexpr int NN = 16; BODY; } break;   \
+    case 32: { constexpr int NN = 32; BODY; } break;   \
+    case 64: { constexpr int NN = 64; BODY; } break;   \
+    case 128: { constexpr int NN = 128; BODY; } break; \
+    case 256: { constexpr int NN = 256; BODY; } break; \
+    case 512: { constexpr int NN = 512; BODY; } break; \
+    case 1024: { constexpr int NN = 1024; BODY; } break; \
+    default: return fail(PS_ERR_UNSUPPORTED, "grid size %d not supported", N); \
+    }
+
 // =========================================================================
 // context
 // =========================================================================
 template <typename T> struct PrecBufs {
-    V2<T>* tw = nullptr;    // W_N^m, m in [0, N)
+    V2<T>* tw = nullptr;    // W_N^m, m in [0, N): r2c / c2r pre- and post-processing
+    V2<T>* twp = nullptr;   // Stockham table of the pencil transforms (length N)
+    V2<T>* twr = nullptr;   // Stockham table of the row transforms (length N/2)
+    Tables<T> tables() const { return Tables<T>{twp, twr, tw}; }
     V2<T>* spec = nullptr;  // field spectrum, row stride S
     V2<T>* work = nullptr;  // work spectrum (band-limited strides <= S)
+    V2<T>* work2 = nullptr; // second and third work spectra (pair groups; allocated on use)
+    V2<T>* work3 = nullptr;
     T* ra = nullptr;        // real grids
     T* rb = nullptr;
     int S = 0;
@@ -81,6 +98,8 @@ struct ps_gpu_ctx {
     size_t dshells_cap = 0;
     unsigned long long* dminmax = nullptr;
     size_t dminmax_cap = 0;
+    unsigned short* dlut = nullptr;  // r2 -> shell bitmask
+    size_t dlut_cap = 0;
     void* stage[2] = {nullptr, nullptr};
     size_t stage_bytes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -109,6 +128,20 @@ int round_up(int a, int b) { return (a + b - 1) / b * b; }
 bool pow2_ok(int n) { return n >= 16 && n <= 1024 && (n & (n - 1)) == 0; }
 double ref_pi() { return acos(-1.0); }  // filter.c:19
 
+// Pencil-tile width (complex elements per row segment) of the pencil kernels.
+template <typename T> int pw(int N)
+{
+    switch (N) {
+    case 16: return PencilGeom<T, 16>::W;
+    case 32: return PencilGeom<T, 32>::W;
+    case 64: return PencilGeom<T, 64>::W;
+    case 128: return PencilGeom<T, 128>::W;
+    case 256: return PencilGeom<T, 256>::W;
+    case 512: return PencilGeom<T, 512>::W;
+    default: return PencilGeom<T, 1024>::W;
+    }
+}
+
 template <typename T> int alloc_dev(T** p, size_t count)
 {
     if (*p) return PS_OK;
@@ -124,10 +157,18 @@ template <typename T> int alloc_dev(T** p, size_t count)
 template <typename T> int init_prec(ps_gpu_ctx* c, PrecBufs<T>& b)
 {
     const int N = c->N;
-    b.S = round_up(N / 2 + 1, PencilWidth<T>::value);
+    b.S = round_up(N / 2 + 1, pw<T>(N));
     const size_t nspec = (size_t)N * N * b.S;
     const size_t nreal = (size_t)N * N * N;
     PS_TRY(alloc_dev(&b.tw, N));
+    PS_TRY(alloc_dev(&b.twp, N));
+    PS_TRY(alloc_dev(&b.twr, N / 2));
+    {
+        std::vector<V2<T>> hp(N), hr(N / 2);
+        PS_SWITCH_N(N, (L3<T, NN>::host_tables(hp.data(), hr.data())));
+        PS_CK(cudaMemcpy(b.twp, hp.data(), sizeof(V2<T>) * N, cudaMemcpyHostToDevice));
+        PS_CK(cudaMemcpy(b.twr, hr.data(), sizeof(V2<T>) * (N / 2), cudaMemcpyHostToDevice));
+    }
     PS_TRY(alloc_dev(&b.spec, nspec));
     PS_TRY(alloc_dev(&b.work, nspec));
     PS_TRY(alloc_dev(&b.ra, nreal));
@@ -146,11 +187,23 @@ template <typename T> int init_prec(ps_gpu_ctx* c, PrecBufs<T>& b)
 template <typename T> void free_prec(PrecBufs<T>& b)
 {
     cudaFree(b.tw);
+    cudaFree(b.twp);
+    cudaFree(b.twr);
     cudaFree(b.spec);
     cudaFree(b.work);
+    cudaFree(b.work2);
+    cudaFree(b.work3);
     cudaFree(b.ra);
     cudaFree(b.rb);
     b = PrecBufs<T>();
+}
+
+template <typename T> int ensure_pair_bufs(ps_gpu_ctx* c, PrecBufs<T>& b)
+{
+    const size_t nspec = (size_t)c->N * c->N * b.S;
+    PS_TRY(alloc_dev(&b.work2, nspec));
+    PS_TRY(alloc_dev(&b.work3, nspec));
+    return PS_OK;
 }
 
 int ensure_partials(ps_gpu_ctx* c, size_t n)
@@ -183,6 +236,16 @@ int ensure_shells(ps_gpu_ctx* c, size_t n)
     c->dshells_cap = n;
     return PS_OK;
 }
+int ensure_lut(ps_gpu_ctx* c, size_t n)
+{
+    if (n <= c->dlut_cap) return PS_OK;
+    cudaFree(c->dlut);
+    c->dlut = nullptr;
+    c->dlut_cap = 0;
+    PS_TRY(alloc_dev(&c->dlut, n));
+    c->dlut_cap = n;
+    return PS_OK;
+}
 int ensure_minmax(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->dminmax_cap) return PS_OK;
@@ -197,18 +260,6 @@ int ensure_minmax(ps_gpu_ctx* c, size_t n)
 // =========================================================================
 // launch plumbing (runtime N -> template N)
 // =========================================================================
-#define PS_SWITCH_N(N, BODY)                       \
-    switch (N) {                                   \
-    case 16: { constexpr int NN = 16; BODY; } break;   \
-    case 32: { constexpr int NN = 32; BODY; } break;   \
-    case 64: { constexpr int NN = 64; BODY; } break;   \
-    case 128: { constexpr int NN = 128; BODY; } break; \
-    case 256: { constexpr int NN = 256; BODY; } break; \
-    case 512: { constexpr int NN = 512; BODY; } break; \
-    case 1024: { constexpr int NN = 1024; BODY; } break; \
-    default: return fail(PS_ERR_UNSUPPORTED, "grid size %d not supported", N); \
-    }
-
 template <typename T> PrecBufs<T>& bufs(ps_gpu_ctx* c);
 template <> PrecBufs<float>& bufs<float>(ps_gpu_ctx* c) { return c->f; }
 template <> PrecBufs<double>& bufs<double>(ps_gpu_ctx* c) { return c->d; }
@@ -226,11 +277,11 @@ namespace {
 // ---------------------------------------------------------------- profiling
 enum KernelFamily {
     KF_FWD_Z = 0, KF_PASS_Y, KF_FWD_X_STORE, KF_FWD_X_DOT, KF_INV_X, KF_INV_Z, KF_SUM, KF_DERIVED,
-    KF_FINAL, KF_COUNT
+    KF_FINAL, KF_PAIR_Z, KF_LUT, KF_COUNT
 };
 const char* const kFamilyName[KF_COUNT] = {"fwd_z_r2c", "pass_y", "fwd_x_store", "fwd_x_dot",
                                            "inv_x_masked", "inv_z_c2r", "sum_partials",
-                                           "derived_range", "finalize"};
+                                           "derived_range", "finalize", "pair_z", "shell_lut"};
 
 int prof_fold(ps_gpu_ctx* c)
 {
@@ -289,34 +340,49 @@ int sum_partials(ps_gpu_ctx* c, int nblocks, int ncols, double* out, int out_str
     return PS_OK;
 }
 
-// Inverse 3D transform of shell-filtered data, band-limited to the shell,
-// with the real-space epilogue.  mode: LOAD_MASKED (F * spectrum) or LOAD_UNIT (F).
-// For reducing epilogues the grid sum lands in *dsum (device).
+// Inverse X and Y passes of a shell-filtered spectrum into dst, band-limited to
+// the shell: h < hb = min(band, N/2) + 1 columns, row stride *S_out.
+// mode: LOAD_MASKED (F * field spectrum) or LOAD_UNIT (F).
+template <typename T>
+int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, int* S_out, int* hb_out)
+{
+    PrecBufs<T>& B = bufs<T>(c);
+    const int N = c->N;
+    const int hb = std::min(band, N / 2) + 1;
+    const int S = round_up(hb, pw<T>(N));
+    const double V = sizeof(V2<T>), NN2 = (double)N * N;
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, dst, S, mode, dshell, N / 2 + 1, B.tables()))));
+        pf.end(KF_INV_X, NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, B.tables()))));
+        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
+    }
+    *S_out = S;
+    *hb_out = hb;
+    return PS_OK;
+}
+
+// Inverse 3D transform of shell-filtered data with the real-space epilogue
+// (store / multiply / reduce x^p * aux).  For reducing epilogues the grid sum
+// lands in *dsum (device).
 template <typename T>
 int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, const T* aux, int epi,
               int power, double* dsum)
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
-    const int hb = std::min(band, N / 2) + 1;
-    const int S = round_up(hb, PencilWidth<T>::value);
     const bool reduce = epi == EPI_MUL_REDUCE || epi == EPI_REDUCE;
     if (reduce) PS_TRY(ensure_partials(c, (size_t)N * N));
-    int nb = 0;
+    int S = 0, hb = 0, nb = 0;
+    PS_TRY(c2r_xy<T>(c, mode, dshell, band, B.work, &S, &hb));
     const double V = sizeof(V2<T>), NN2 = (double)N * N;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, B.work, S, mode, dshell, N / 2 + 1, B.tw))));
-        pf.end(KF_INV_X, NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
-    }
-    {
-        Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, true, B.tw))));
-        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
-    }
-    {
-        Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_z(c->stream, B.work, S, hb, out, aux, epi, power, c->partials, B.tw, &nb))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_z(c->stream, B.work, S, hb, out, aux, epi, power, c->partials, B.tables(), &nb))));
         const double real = NN2 * N * sizeof(T);
         const double extra = (epi == EPI_STORE ? real : 0.0) + (epi == EPI_MUL_STORE ? 2.0 * real : 0.0) +
                              (epi == EPI_MUL_REDUCE ? real : 0.0);
@@ -327,6 +393,30 @@ int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, co
     return PS_OK;
 }
 
+// Spectrum of the real product of two band-limited inverse transforms (B may be
+// NULL: square of A), rows kept to h < hout, forward Y pass done; into B.work3.
+template <typename T>
+int pair_spectrum(ps_gpu_ctx* c, const V2<T>* A, int Sa, int hba, const V2<T>* Bq, int Sb, int hbb, int hout,
+                  int* S_out)
+{
+    PrecBufs<T>& B = bufs<T>(c);
+    const int N = c->N;
+    const int S = round_up(hout, pw<T>(N));
+    const double V = sizeof(V2<T>), NN2 = (double)N * N;
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, B.tables()))));
+        pf.end(KF_PAIR_Z, NN2 * (hba + (Bq ? hbb : 0) + hout) * V);
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, B.tables()))));
+        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
+    }
+    *S_out = S;
+    return PS_OK;
+}
+
 // Forward transform of a real grid into B.work (row stride returned), rows
 // truncated to h < hout.
 template <typename T>
@@ -334,17 +424,17 @@ int r2c_work(ps_gpu_ctx* c, int kind, const void* a, const void* b, int hout, in
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
-    const int S = round_up(hout, PencilWidth<T>::value);
+    const int S = round_up(hout, pw<T>(N));
     const double V = sizeof(V2<T>), NN2 = (double)N * N;
     const double src_bytes = kind == SRC_T ? sizeof(T) : (kind == SRC_F32 ? 4.0 : kind == SRC_F64 ? 8.0 : kind == SRC_XHI_F32 ? 8.0 : 16.0);
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.work, S, hout, B.tw))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.work, S, hout, B.tables()))));
         pf.end(KF_FWD_Z, NN2 * N * src_bytes + NN2 * hout * V);
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, false, B.tw))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, false, B.tables()))));
         pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
     }
     *stride_out = S;
@@ -361,18 +451,18 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     const double src_bytes = kind == SRC_F32 ? 4.0 : kind == SRC_F64 ? 8.0 : kind == SRC_XHI_F32 ? 8.0 : 16.0;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, N / 2 + 1, B.tw))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, N / 2 + 1, B.tables()))));
         pf.end(KF_FWD_Z, NN2 * N * src_bytes + NN2 * H * V);
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tw))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tables()))));
         pf.end(KF_PASS_Y, 2.0 * NN2 * B.S * V);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.spec, B.S, N / 2 + 1, epi, B.spec, B.S, nullptr, 0,
-                                                nullptr, 0, nullptr, B.tw, nullptr))));
+                                                nullptr, 0, nullptr, 0, nullptr, B.tables(), nullptr))));
         pf.end(KF_FWD_X_STORE, 2.0 * NN2 * H * V);
     }
     PS_CK(cudaGetLastError());
@@ -382,20 +472,37 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
 
 // Dot / count pass over a forward-transformed work buffer (stride S, band
 // hvalid) for up to MAX_DOT_SHELLS shells per launch; results to dout[0..ns).
+// hsh: host copies of the shells (decide whether an r2 bitmask table applies).
 template <typename T>
-int dot_pass(ps_gpu_ctx* c, int epi, int S, int hvalid, const Shell* dshells, int ns, double* dout)
+int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell* dshells,
+             const Shell* hsh, int ns, double* dout)
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
     for (int s0 = 0; s0 < ns; s0 += MAX_DOT_SHELLS) {
         const int cnt = std::min(MAX_DOT_SHELLS, ns - s0);
-        const size_t blocks = (size_t)N * (S / PencilWidth<T>::value);
+        const size_t blocks = (size_t)N * (S / pw<T>(N));
         PS_TRY(ensure_partials(c, blocks * MAX_DOT_SHELLS));
+        bool lut_ok = true;
+        int lut_size = 0;
+        for (int q = s0; q < s0 + cnt; q++) {
+            if (hsh[q].kind != SHELL_DEFAULT && hsh[q].kind != SHELL_RANGE) lut_ok = false;
+            lut_size = std::max(lut_size, hsh[q].r2hi + 1);
+        }
+        const unsigned short* lut = nullptr;
+        if (lut_ok) {
+            PS_TRY(ensure_lut(c, (size_t)std::max(lut_size, 1)));
+            Prof pf(c);
+            if (lut_size > 0)
+                k_shell_lut<<<(lut_size + 255) / 256, 256, 0, c->stream>>>(dshells + s0, cnt, lut_size, c->dlut);
+            pf.end(KF_LUT, 2.0 * lut_size);
+            lut = c->dlut;
+        }
         int nb = 0;
         {
             Prof pf(c);
-            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.work, S, hvalid, epi, nullptr, 0, B.spec, B.S,
-                                                    dshells + s0, cnt, c->partials, B.tw, &nb))));
+            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, data, S, hvalid, epi, nullptr, 0, B.spec, B.S,
+                                                    dshells + s0, cnt, lut, lut_size, c->partials, B.tables(), &nb))));
             pf.end(KF_FWD_X_DOT, (double)N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
         }
         PS_TRY(sum_partials(c, nb, cnt, dout + s0, 1));
@@ -443,6 +550,9 @@ Shell make_shell(int kind, double k, double kmin, double kmax, double binwidth, 
     default: rb = std::max(s.mmin, s.mmax) + 1.7320508075688772 * ah + 1e-9; break;
     }
     s.band = band_of(rb, N);
+    shell_r2_interval(s, N);
+    if (kind == SHELL_DEFAULT || kind == SHELL_RANGE)  // |m_x| <= sqrt(r2) <= sqrt(r2hi)
+        s.band = std::min(s.band, s.r2hi >= 0 ? (int)floor(sqrt((double)s.r2hi)) : 0);
     return s;
 }
 
@@ -733,6 +843,10 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
     PS_CK(cudaMemcpyAsync(c->dshells, table.data(), sizeof(Shell) * table.size(),
                           cudaMemcpyHostToDevice, c->stream));
     PS_TRY(ensure_sums(c, 4 * (size_t)nconf + 8));
+    if (!groups.empty()) {
+        PS_TRY(ensure_pair_bufs(c, c->f));
+        PS_TRY(ensure_pair_bufs(c, c->d));
+    }
     double* sumD = c->dsums;
     double* sumI = c->dsums + nconf;  // exact counts (count mode)
     std::vector<double> coef(nconf);
@@ -750,31 +864,18 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
         // scratch sums for the group, then scatter
         double* gD = c->dsums + 2 * nconf;
         double* gI = c->dsums + 3 * nconf;
-        // D part (FP32): P = D_a * D_b, transform, dot with dk over each closing shell
-        if (G.a == G.b) {
-            PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + G.a, sa.band, c->f.rb, nullptr, EPI_STORE, 2,
-                                    nullptr));
-        } else {
-            PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + G.a, sa.band, c->f.ra, nullptr, EPI_STORE, 1,
-                                    nullptr));
-            PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + G.b, sb.band, c->f.rb, c->f.ra,
-                                    EPI_MUL_STORE, 1, nullptr));
-        }
-        int S = 0;
-        PS_TRY(r2c_work<float>(c, SRC_T, c->f.rb, nullptr, hout, &S));
-        PS_TRY(dot_pass<float>(c, SPEC_DOT, S, hout, c->dshells + gofs[g], ng, gD));
-        // I part (FP64): counts
-        if (G.a == G.b) {
-            PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.rb, nullptr, EPI_STORE, 2,
-                                     nullptr));
-        } else {
-            PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.ra, nullptr, EPI_STORE, 1,
-                                     nullptr));
-            PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + G.b, sb.band, c->d.rb, c->d.ra,
-                                     EPI_MUL_STORE, 1, nullptr));
-        }
-        PS_TRY(r2c_work<double>(c, SRC_T, c->d.rb, nullptr, hout, &S));
-        PS_TRY(dot_pass<double>(c, SPEC_COUNT, S, hout, c->dshells + gofs[g], ng, gI));
+        // D part (FP32): P = D_a * D_b formed row by row and transformed back,
+        // then one masked dot product with dk per closing shell
+        int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
+        PS_TRY(c2r_xy<float>(c, LOAD_MASKED, c->dshells + G.a, sa.band, c->f.work, &Sa, &ha));
+        if (G.a != G.b) PS_TRY(c2r_xy<float>(c, LOAD_MASKED, c->dshells + G.b, sb.band, c->f.work2, &Sb, &hbb));
+        PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout, &S));
+        PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gD));
+        // I part (FP64): the same on unit shells, counts rounded per mode
+        PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.work, &Sa, &ha));
+        if (G.a != G.b) PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.b, sb.band, c->d.work2, &Sb, &hbb));
+        PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S));
+        PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gI));
         for (int x = 0; x < ng; x++) {
             PS_CK(cudaMemcpyAsync(sumD + G.cfg[x], gD + x, 8, cudaMemcpyDeviceToDevice, c->stream));
             PS_CK(cudaMemcpyAsync(sumI + G.cfg[x], gI + x, 8, cudaMemcpyDeviceToDevice, c->stream));
@@ -1175,6 +1276,7 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     cudaFree(c->dsums);
     cudaFree(c->dshells);
     cudaFree(c->dminmax);
+    cudaFree(c->dlut);
     cudaFree(c->stage[0]);
     cudaFree(c->stage[1]);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);

@@ -42,6 +42,8 @@ enum ShellKind : int {
 struct Shell {
     int kind;
     int band;      // every selected mode has |m_x|,|m_y|,|m_z| <= band (host bound)
+    int r2lo;      // DEFAULT / RANGE: selected <=> r2lo <= mx^2+my^2+mz^2 <= r2hi
+    int r2hi;
     double kk;     // k/(2 pi)*L           (DEFAULT, WATKINSON)
     double mmin;   // kmin/(2 pi)*L        (RANGE kinds)
     double mmax;   // kmax/(2 pi)*L        (RANGE kinds)
@@ -75,16 +77,63 @@ __device__ __forceinline__ void corners_fold(int mx, int my, int mz, double e, d
     }
 }
 
+// The DEFAULT and RANGE predicates (filter.c:57-59, :155-158) depend on the
+// integer r2 = mx^2+my^2+mz^2 only, through s = fl(sqrt(r2)), which is
+// non-decreasing in r2; each is a conjunction of one condition that is
+// monotone false->true in s and one that is monotone true->false (fl(a - s)
+// is non-increasing in s).  So the selected r2 form one integer interval,
+// found by binary search with the exact FP64 predicate (same operations as
+// the reference, correctly rounded sqrt on host and device alike).
+__host__ __device__ inline double exact_sqrt(double x)
+{
+#ifdef __CUDA_ARCH__
+    return __dsqrt_rn(x);
+#else
+    return sqrt(x);
+#endif
+}
+__host__ __device__ inline bool pred_lower(const Shell& s, int r2)  // monotone false -> true
+{
+    const double m = exact_sqrt((double)r2);
+    return s.kind == SHELL_DEFAULT ? (s.kk - m <= s.half) : (s.mmin - m <= s.half);
+}
+__host__ __device__ inline bool pred_upper(const Shell& s, int r2)  // monotone true -> false
+{
+    const double m = exact_sqrt((double)r2);
+    return s.kind == SHELL_DEFAULT ? (s.kk - m >= -s.half) : (m - s.mmax <= s.half);
+}
+// fabs(kk - m) <= half  <=>  -half <= fl(kk - m) <= half (fabs and negation are exact).
+__host__ __device__ inline void shell_r2_interval(Shell& s, int n)
+{
+    if (s.kind != SHELL_DEFAULT && s.kind != SHELL_RANGE) {
+        s.r2lo = 0;
+        s.r2hi = 0x7fffffff;
+        return;
+    }
+    const int r2max = 3 * (n / 2) * (n / 2);
+    int lo = 0, hi = r2max + 1;  // first r2 with pred_lower (r2max+1: none)
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (pred_lower(s, mid)) hi = mid;
+        else lo = mid + 1;
+    }
+    int a = -1, b = r2max;  // last r2 with pred_upper (-1: none)
+    while (a < b) {
+        const int mid = a + (b - a + 1) / 2;
+        if (pred_upper(s, mid)) a = mid;
+        else b = mid - 1;
+    }
+    s.r2lo = lo;
+    s.r2hi = a;
+}
+
 __device__ __forceinline__ bool shell_bit(const Shell& s, int mx, int my, int mz)
 {
     switch (s.kind) {
-    case SHELL_DEFAULT: {
-        const double m = __dsqrt_rn((double)(mx * mx + my * my + mz * mz));
-        return fabs(__dsub_rn(s.kk, m)) <= s.half;
-    }
+    case SHELL_DEFAULT:
     case SHELL_RANGE: {
-        const double m = __dsqrt_rn((double)(mx * mx + my * my + mz * mz));
-        return __dsub_rn(s.mmin, m) <= s.half && __dsub_rn(m, s.mmax) <= s.half;
+        const int r2 = mx * mx + my * my + mz * mz;
+        return r2 >= s.r2lo && r2 <= s.r2hi;
     }
     case SHELL_WATKINSON: {
         double min2 = s.min2_init, max2 = 0.0;

@@ -93,6 +93,14 @@ template <int N, int R> struct RadixPlan {
         for (int q = 0; q < p; q++) s *= radix(q);
         return s;
     }
+    // offset of pass p's twiddles in the Stockham table (entries [k][q-1],
+    // k < span(p), q in [1, radix(p))); the table has N - 1 entries in all
+    __host__ __device__ static constexpr int tw_off(int p)
+    {
+        int o = 0;
+        for (int q = 0; q < p; q++) o += span(q) * (radix(q) - 1);
+        return o;
+    }
     static_assert(R >= 2 && (R & (R - 1)) == 0, "radix must be a power of two");
     static_assert((N & (N - 1)) == 0 && N >= R, "length must be a power of two >= R");
 };
@@ -102,10 +110,28 @@ template <int N> struct DefaultRadix {
     static constexpr int value = N <= 16 ? N : (N == 32 || N == 64 || N == 128 || N == 512) ? 8 : 16;
 };
 
-// tw[m] = W_{TWN}^m = exp(-2 pi i m / TWN); a transform of length N uses
-// W_N^m = tw[m * (TWN / N)].
-template <typename V, int N, int R, bool INV, int TWN, int P_ = 0, class Acc>
-__device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* __restrict__ tw)
+// Synchronisation between passes: the whole CTA (pencil kernels, whose
+// transforms span several warps), or only the threads of one row (row
+// kernels): __syncwarp when a row lives in one warp, else a named barrier per
+// row (ids 1..15; id 0 is __syncthreads').
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+template <int TPF> struct RowSync {
+    int bar;
+    __device__ __forceinline__ void operator()() const
+    {
+        if constexpr (TPF <= 32) __syncwarp();
+        else asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(TPF) : "memory");
+    }
+};
+
+// Stockham passes.  twt is the transform's twiddle table: for pass p, entry
+// tw_off(p) + k*(Rp-1) + (q-1) = W_{Ns*Rp}^{q*k} (forward sign), so the lanes
+// of a warp (consecutive k) read it with a stride of Rp-1 entries, which maps
+// 8 (FP64) or 16 (FP32) consecutive lanes to distinct shared-memory banks.
+template <typename V, int N, int R, bool INV, int P_ = 0, class Acc, class Sync>
+__device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* __restrict__ twt, const Sync& sync)
 {
     using Plan = RadixPlan<N, R>;
     if constexpr (P_ < Plan::P) {
@@ -113,7 +139,6 @@ __device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* _
         constexpr int Ns = Plan::span(P_);
         constexpr int BPT = R / Rp;
         constexpr int TPF = N / R;
-        constexpr int TWS = (N / (Ns * Rp)) * (TWN / N);
         constexpr bool LAST = (P_ == Plan::P - 1);
 #pragma unroll
         for (int u = 0; u < BPT; u++) {
@@ -123,9 +148,10 @@ __device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* _
             const int v = t + TPF * u;
             const int k = v & (Ns - 1);
             if constexpr (Ns > 1) {
+                const V* tp = twt + Plan::tw_off(P_) + k * (Rp - 1);
 #pragma unroll
                 for (int q = 1; q < Rp; q++) {
-                    V w = tw[q * k * TWS];
+                    V w = tp[q - 1];
                     if constexpr (INV) w.y = -w.y;
                     b[q] = cmul(b[q], w);
                 }
@@ -141,12 +167,30 @@ __device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* _
             }
         }
         if constexpr (!LAST) {
-            __syncthreads();
+            sync();
 #pragma unroll
             for (int e = 0; e < R; e++) a[e] = sm.ld(t + TPF * e);
-            __syncthreads();
-            fft_passes<V, N, R, INV, TWN, P_ + 1>(a, t, sm, tw);
+            sync();
+            fft_passes<V, N, R, INV, P_ + 1>(a, t, sm, twt, sync);
         }
+    }
+}
+
+// Host side: the Stockham table of RadixPlan<N, R> (forward sign), from
+// exp(-2 pi i m / M) evaluated in long double.
+template <typename V, int N, int R> inline void stockham_table(V* out)
+{
+    using Plan = RadixPlan<N, R>;
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int p = 0; p < Plan::P; p++) {
+        const int Rp = Plan::radix(p), Ns = Plan::span(p);
+        V* tp = out + Plan::tw_off(p);
+        for (int k = 0; k < Ns; k++)
+            for (int q = 1; q < Rp; q++) {
+                const long double a = two_pi * (long double)(q * k) / (long double)(Ns * Rp);
+                tp[k * (Rp - 1) + q - 1].x = (decltype(tp->x))cosl(a);
+                tp[k * (Rp - 1) + q - 1].y = (decltype(tp->x))(-sinl(a));
+            }
     }
 }
 
@@ -160,11 +204,18 @@ template <typename V, int W> struct SmemInterleaved {
     __device__ __forceinline__ V ld(int pos) const { return s[pos * W + lane]; }
 };
 
-// Shared-memory accessor for row passes: one padded row per transform.
+// Shared-memory accessor for row passes: one row per transform, XOR-swizzled
+// within 128-byte groups: element pos lives at pos ^ ((pos >> LB) & (G-1)),
+// G = 2^LB elements per 128 bytes.  Stockham writes of stride Rp (and 2, 4
+// interleaved runs) then hit G distinct bank groups per 128-byte wavefront,
+// and reads of consecutive positions stay conflict-free.
 template <typename V> struct SmemRow {
+    static constexpr int LB = sizeof(V) == 16 ? 3 : 4;
+    static constexpr int G = 1 << LB;
     V* s;
-    __device__ __forceinline__ void st(int pos, V v) { s[pos + (pos >> 5)] = v; }
-    __device__ __forceinline__ V ld(int pos) const { return s[pos + (pos >> 5)]; }
+    __device__ __forceinline__ static int phys(int pos) { return pos ^ ((pos >> LB) & (G - 1)); }
+    __device__ __forceinline__ void st(int pos, V v) { s[phys(pos)] = v; }
+    __device__ __forceinline__ V ld(int pos) const { return s[phys(pos)]; }
 };
 
 }  // namespace ps

@@ -11,11 +11,16 @@
 //   pass_y : along j for every (i,h) pencil, in place
 //   inv_z  : c2r along l for every (i,j) row; epilogue stores / multiplies /
 //            reduces the real field
+//   pair_z : c2r of two rows, product, r2c of the product (pair groups)
 // Forward 3D transform (r2c, unnormalised like FFTW_FORWARD, fft.c:32):
 //   fwd_z  : r2c along l, loader composes the input field
 //   pass_y : along j
 //   fwd_x  : along i; epilogue stores the spectrum (optionally phase only) or
 //            folds it into per-shell dot products
+//
+// Every kernel stages the twiddle table W_N^m (m < N) in shared memory first;
+// row kernels synchronise per row (warp or named barrier), pencil kernels per
+// CTA (a pencil's threads span several warps).
 #pragma once
 
 #include "ps_common.cuh"
@@ -27,29 +32,85 @@ constexpr int MAX_DOT_SHELLS = 16;
 
 // Pencils per CTA in the strided passes: one 128-byte segment of a row.
 template <typename T> struct PencilWidth { static constexpr int value = 128 / (int)sizeof(V2<T>); };
-// Rows per CTA in the contiguous-axis passes.
-template <typename T, int N> struct RowsPerCta {
-    static constexpr int NH = N / 2;
-    static constexpr int TPF = NH / DefaultRadix<NH>::value;
-    static constexpr int value = TPF >= 64 ? 4 : (TPF >= 16 ? 8 : (TPF >= 4 ? 16 : 32));
+
+// Elements per thread of the pencil (strided-axis) transforms: radix 16 for
+// FP32 at N = 512 so a CTA of 16 pencils is 512 threads.
+template <typename T, int N> struct PencilRadix {
+    static constexpr int value = (sizeof(T) == 4 && N == 512) ? 16 : DefaultRadix<N>::value;
+};
+template <typename T, int N> struct PencilGeom {
+    static constexpr int R = PencilRadix<T, N>::value;
+    static constexpr int TPF = N / R;
+    // one 128-byte segment per row, whole warps per CTA, at most 512 threads
+    // (so an epilogue keeps 16 FP64 accumulators in registers)
+    static constexpr int W0 = PencilWidth<T>::value * TPF >= 32 ? PencilWidth<T>::value : 32 / TPF;
+    static constexpr int W = W0 * TPF > 512 ? 512 / TPF : W0;
+    static constexpr int THREADS = TPF * W;
+    static constexpr size_t TW_BYTES = (size_t)N * sizeof(V2<T>);  // Stockham table (N-1 used)
+    static constexpr size_t SMEM = TW_BYTES + (size_t)N * W * sizeof(V2<T>);
 };
 
-template <typename T, int N> struct PencilGeom {
-    static constexpr int R = DefaultRadix<N>::value;
-    static constexpr int TPF = N / R;
-    static constexpr int W = PencilWidth<T>::value;
-    static constexpr int THREADS = TPF * W;
-    static constexpr size_t SMEM = (size_t)N * W * sizeof(V2<T>);
+// Elements per thread of the row (contiguous-axis) transforms of length NH:
+// at most 32 threads per row (warp-synchronous) except FP64 rows of 512,
+// which use radix 8 and 64 threads (two transforms must fit in registers).
+template <typename T, int NH> struct RowRadix {
+    static constexpr int value = NH <= 16 ? NH : ((sizeof(T) == 4 && NH == 512) ? 16 : 8);
 };
 template <typename T, int N> struct RowGeom {
     static constexpr int NH = N / 2;
-    static constexpr int R = DefaultRadix<NH>::value;
+    static constexpr int R = RowRadix<T, NH>::value;
     static constexpr int TPF = NH / R;
-    static constexpr int WZ = RowsPerCta<T, N>::value;
+    static constexpr int WZ = (256 / TPF) < 32 ? (256 / TPF) : 32;  // rows per CTA (tile)
     static constexpr int THREADS = TPF * WZ;
-    static constexpr int ROW = NH + NH / 32 + 2;  // padded row (>= NH+1)
-    static constexpr size_t SMEM = (size_t)ROW * WZ * sizeof(V2<T>);
+    static constexpr int EPC = 16 / (int)sizeof(V2<T>);  // complex elements per 16-byte copy
+    // shared memory: row Stockham table [NH], pre/post twiddles W_N^k, k <= NH
+    // [NH+2], per-row exchange buffers [WZ][NH], then the input stages
+    static constexpr size_t TWR_OFF = 0;
+    static constexpr size_t TWPP_OFF = TWR_OFF + (size_t)NH * sizeof(V2<T>);
+    static constexpr size_t ROWBUF_OFF = TWPP_OFF + (size_t)(NH + 2) * sizeof(V2<T>);
+    static constexpr size_t STAGE_OFF = ROWBUF_OFF + (size_t)WZ * NH * sizeof(V2<T>);
+    // input stage pitch (elements) for rows of hv valid entries
+    __host__ __device__ static constexpr int pitch(int hv) { return (hv + EPC - 1) / EPC * EPC; }
+    // dynamic shared memory of a kernel with `ninputs` double-buffered inputs
+    __host__ __device__ static constexpr size_t smem(int ninputs, int hva, int hvb)
+    {
+        return STAGE_OFF + (size_t)2 * WZ * (pitch(hva) + (ninputs > 1 ? pitch(hvb) : 0)) * sizeof(V2<T>);
+    }
+    static_assert(TPF <= 32 || WZ <= 15, "one named barrier per row");
 };
+
+// Copy a twiddle table into shared memory (whole CTA).
+template <typename V>
+__device__ __forceinline__ V* stage_table(unsigned char* smem, const V* __restrict__ src, int n)
+{
+    V* dst = reinterpret_cast<V*>(smem);
+    for (int q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[q];
+    return dst;
+}
+
+// cp.async (16-byte, L2-only) copies global -> shared, grouped; the waits are
+// the hardware's own (no polling loop in this code).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Stage WZ consecutive spectrum rows (first hv entries, rounded up to a
+// 16-byte multiple, which stays inside the row stride ss) into `stage`
+// (pitch P) with the whole CTA.
+template <typename V, int WZ, int THREADS>
+__device__ __forceinline__ void stage_rows(V* stage, int P, const V* __restrict__ src, size_t row0, int ss, int hv)
+{
+    constexpr int EPC = 16 / (int)sizeof(V);
+    const int chunks = (hv + EPC - 1) / EPC;
+    for (int c = threadIdx.x; c < WZ * chunks; c += THREADS) {
+        const int w = c / chunks, q = c - w * chunks;
+        cp_async16(stage + w * P + q * EPC, src + (row0 + w) * ss + q * EPC);
+    }
+}
 
 // ------------------------------------------------------------------ reductions
 // Deterministic block sum: fixed shuffle tree, then warp partials in order.
@@ -76,12 +137,14 @@ enum InvLoad : int { LOAD_PLAIN = 0, LOAD_MASKED = 1, LOAD_UNIT = 2 };
 template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     k_inv_x(const V2<T>* __restrict__ src, int src_stride, V2<T>* __restrict__ dst, int dst_stride,
-            int mode, const Shell* __restrict__ shell_p, int hvalid, const V2<T>* __restrict__ tw)
+            int mode, const Shell* __restrict__ shell_p, int hvalid, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw), (int)(threadIdx.x % G::W)};
+    const V* tw = stage_table<V>(smem_raw, tw_g, N);
+    __syncthreads();
+    SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), (int)(threadIdx.x % G::W)};
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
     const int tiles_per_row = dst_stride / G::W;
     const int j = blockIdx.x / tiles_per_row;
@@ -117,7 +180,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
         }
         a[e] = v;
     }
-    fft_passes<V, N, G::R, true, N>(a, t, sm, tw);
+    fft_passes<V, N, G::R, true>(a, t, sm, tw, BlockSync{});
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int i = t + G::TPF * e;
@@ -128,12 +191,11 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 // ------------------------------------------------------------------ Y pass
 template <typename T, int N, bool INV>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
-    k_pass_y(V2<T>* __restrict__ data, int stride, const V2<T>* __restrict__ tw)
+    k_pass_y(V2<T>* __restrict__ data, int stride, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw), (int)(threadIdx.x % G::W)};
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
     const int tiles_per_plane = stride / G::W;
     const int i = blockIdx.x / tiles_per_plane;
@@ -142,9 +204,85 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     V a[G::R];
 #pragma unroll
     for (int e = 0; e < G::R; e++) a[e] = base[(size_t)(t + G::TPF * e) * stride];
-    fft_passes<V, N, G::R, INV, N>(a, t, sm, tw);
+    const V* tw = stage_table<V>(smem_raw, tw_g, N);
+    __syncthreads();
+    SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), w};
+    fft_passes<V, N, G::R, INV>(a, t, sm, tw, BlockSync{});
 #pragma unroll
     for (int e = 0; e < G::R; e++) base[(size_t)(t + G::TPF * e) * stride] = a[e];
+}
+
+// ------------------------------------------------------------------ row helpers
+// A CTA works on tiles of WZ consecutive (i,j) rows; row w of a tile is done
+// by threads [w*TPF, (w+1)*TPF), which synchronise among themselves only.
+template <typename T, int N> struct RowCtx {
+    using G = RowGeom<T, N>;
+    using V = V2<T>;
+    int w, t;
+    V* rowbuf;       // this row's exchange buffer [NH]
+    const V* twr;    // Stockham table of the NH-point transform
+    const V* twpp;   // W_N^k, k <= NH (r2c / c2r pre- and post-processing)
+    RowSync<G::TPF> sync;
+    // stage both tables (caller issues the __syncthreads that publishes them)
+    __device__ __forceinline__ RowCtx(unsigned char* smem, const V* __restrict__ twr_g,
+                                      const V* __restrict__ twpp_g)
+    {
+        twr = stage_table<V>(smem + G::TWR_OFF, twr_g, G::NH);
+        twpp = stage_table<V>(smem + G::TWPP_OFF, twpp_g, G::NH + 1);
+        w = threadIdx.x / G::TPF;
+        t = threadIdx.x % G::TPF;
+        rowbuf = reinterpret_cast<V*>(smem + G::ROWBUF_OFF) + w * G::NH;
+        sync.bar = 1 + w;
+    }
+};
+
+// c2r of one spectrum row held in shared memory (entries h < hv, zero above)
+// into registers, canonical layout: a[e] = (x[2n], x[2n+1]), n = t + TPF*e.
+template <typename T, int N>
+__device__ __forceinline__ void c2r_row(const V2<T>* zr, int hv, RowCtx<T, N>& rc,
+                                        V2<T> (&a)[RowGeom<T, N>::R])
+{
+    using G = RowGeom<T, N>;
+    using V = V2<T>;
+    constexpr int NH = G::NH;
+#pragma unroll
+    for (int e = 0; e < G::R; e++) {
+        const int k = rc.t + G::TPF * e;
+        const V zk = k < hv ? zr[k] : czero<V>();
+        const V zm = (NH - k) < hv ? cconj(zr[NH - k]) : czero<V>();
+        const V A = cadd(zk, zm);
+        const V B = cmul(csub(zk, zm), cconj(rc.twpp[k]));  // exp(+2 pi i k / N)
+        a[e] = V{A.x - B.y, A.y + B.x};
+    }
+    SmemRow<V> sm{rc.rowbuf};
+    fft_passes<V, NH, G::R, true>(a, rc.t, sm, rc.twr, rc.sync);
+    rc.sync();
+}
+
+// r2c of a real row held in registers (canonical pairs), writing h < hout.
+template <typename T, int N>
+__device__ __forceinline__ void r2c_row(V2<T> (&a)[RowGeom<T, N>::R], RowCtx<T, N>& rc, V2<T>* __restrict__ xo,
+                                        int hout)
+{
+    using G = RowGeom<T, N>;
+    using V = V2<T>;
+    constexpr int NH = G::NH;
+    SmemRow<V> sm{rc.rowbuf};
+    fft_passes<V, NH, G::R, false>(a, rc.t, sm, rc.twr, rc.sync);
+    rc.sync();
+#pragma unroll
+    for (int e = 0; e < G::R; e++) sm.st(rc.t + G::TPF * e, a[e]);
+    rc.sync();
+    const T half = (T)0.5;
+    for (int k = rc.t; k <= NH && k < hout; k += G::TPF) {
+        const V yk = sm.ld(k & (NH - 1));
+        const V ym = cconj(sm.ld((NH - k) & (NH - 1)));
+        const V E = V{(yk.x + ym.x) * half, (yk.y + ym.y) * half};
+        const V D = csub(yk, ym);
+        const V O = V{D.y * half, -D.x * half};  // D / (2i)
+        xo[k] = cadd(E, cmul(rc.twpp[k], O));
+    }
+    rc.sync();
 }
 
 // ------------------------------------------------------------------ inverse Z (c2r)
@@ -162,53 +300,56 @@ template <typename T> __device__ __forceinline__ T ipow(T x, int p)
     return r;
 }
 
+// Persistent: CTA b handles tiles b, b + gridDim.x, ...; the next tile's rows
+// are copied into the other stage buffer while the current one is computed.
 template <typename T, int N>
 __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
     k_inv_z(const V2<T>* __restrict__ src, int src_stride, int hvalid, T* out, const T* aux,
-            int epi, int power, double* __restrict__ partials, const V2<T>* __restrict__ tw)
+            int epi, int power, double* __restrict__ partials, const V2<T>* __restrict__ twr_g,
+            const V2<T>* __restrict__ twpp_g)
 {
     using G = RowGeom<T, N>;
     using V = V2<T>;
-    constexpr int NH = G::NH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[(G::THREADS + 31) / 32];
-    const int w = threadIdx.x / G::TPF, t = threadIdx.x % G::TPF;
-    V* srow = reinterpret_cast<V*>(smem_raw) + w * G::ROW;
-    const size_t row = (size_t)blockIdx.x * G::WZ + w;
-    const V* zr = src + row * src_stride;
-    for (int hh = t; hh <= NH; hh += G::TPF) srow[hh] = hh < hvalid ? zr[hh] : czero<V>();
-    __syncthreads();
-    V a[G::R];
-#pragma unroll
-    for (int e = 0; e < G::R; e++) {
-        const int k = t + G::TPF * e;
-        const V zk = srow[k];
-        const V zm = cconj(srow[NH - k]);
-        const V A = cadd(zk, zm);
-        const V B = cmul(csub(zk, zm), cconj(tw[k]));  // exp(+2 pi i k / N)
-        a[e] = V{A.x - B.y, A.y + B.x};
-    }
-    __syncthreads();
-    SmemRow<V> sm{srow};
-    fft_passes<V, NH, G::R, true, N>(a, t, sm, tw);
+    RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
+    const int P = G::pitch(hvalid);
+    V* stage = reinterpret_cast<V*>(smem_raw + G::STAGE_OFF);
+    const int ntiles = N * N / G::WZ;
+    int tile = blockIdx.x;
+    if (tile < ntiles) stage_rows<V, G::WZ, G::THREADS>(stage, P, src, (size_t)tile * G::WZ, src_stride, hvalid);
+    cp_async_commit();
     double acc = 0.0;
-    T* orow = out ? out + row * N : nullptr;
-    const T* arow = aux ? aux + row * N : nullptr;
+    for (int st = 0; tile < ntiles; tile += gridDim.x, st ^= 1) {
+        const int next = tile + gridDim.x;
+        if (next < ntiles)
+            stage_rows<V, G::WZ, G::THREADS>(stage + (st ^ 1) * G::WZ * P, P, src, (size_t)next * G::WZ,
+                                             src_stride, hvalid);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();
+        const size_t row = (size_t)tile * G::WZ + rc.w;
+        V a[G::R];
+        c2r_row<T, N>(stage + st * G::WZ * P + rc.w * P, hvalid, rc, a);
+        T* orow = out ? out + row * N : nullptr;
+        const T* arow = aux ? aux + row * N : nullptr;
 #pragma unroll
-    for (int e = 0; e < G::R; e++) {
-        const int n2 = 2 * (t + G::TPF * e);
-        T x0 = ipow(a[e].x, power), x1 = ipow(a[e].y, power);
-        if (epi == EPI_STORE) {
-            *reinterpret_cast<V*>(orow + n2) = V{x0, x1};
-        } else if (epi == EPI_MUL_STORE) {
-            const V q = *reinterpret_cast<const V*>(arow + n2);
-            *reinterpret_cast<V*>(orow + n2) = V{x0 * q.x, x1 * q.y};
-        } else if (epi == EPI_MUL_REDUCE) {
-            const V q = *reinterpret_cast<const V*>(arow + n2);
-            acc += (double)x0 * (double)q.x + (double)x1 * (double)q.y;
-        } else {
-            acc += (double)x0 + (double)x1;
+        for (int e = 0; e < G::R; e++) {
+            const int n2 = 2 * (rc.t + G::TPF * e);
+            T x0 = ipow(a[e].x, power), x1 = ipow(a[e].y, power);
+            if (epi == EPI_STORE) {
+                *reinterpret_cast<V*>(orow + n2) = V{x0, x1};
+            } else if (epi == EPI_MUL_STORE) {
+                const V q = *reinterpret_cast<const V*>(arow + n2);
+                *reinterpret_cast<V*>(orow + n2) = V{x0 * q.x, x1 * q.y};
+            } else if (epi == EPI_MUL_REDUCE) {
+                const V q = *reinterpret_cast<const V*>(arow + n2);
+                acc += (double)x0 * (double)q.x + (double)x1 * (double)q.y;
+            } else {
+                acc += (double)x0 + (double)x1;
+            }
         }
+        __syncthreads();  // stage st is refilled two tiles later
     }
     if (epi == EPI_MUL_REDUCE || epi == EPI_REDUCE) {
         const double s = block_sum<G::THREADS>(acc, red);
@@ -246,45 +387,87 @@ __device__ __forceinline__ T load_real(int kind, const void* a, const void* b, s
     }
 }
 
+// One tile per CTA (the input rows are dense and all loads are issued up front).
 template <typename T, int N>
 __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
     k_fwd_z(int kind, const void* __restrict__ a_src, const void* __restrict__ b_src,
-            V2<T>* __restrict__ dst, int dst_stride, int hout, const V2<T>* __restrict__ tw)
+            V2<T>* __restrict__ dst, int dst_stride, int hout, const V2<T>* __restrict__ twr_g,
+            const V2<T>* __restrict__ twpp_g)
 {
     using G = RowGeom<T, N>;
     using V = V2<T>;
-    constexpr int NH = G::NH;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int w = threadIdx.x / G::TPF, t = threadIdx.x % G::TPF;
-    V* srow = reinterpret_cast<V*>(smem_raw) + w * G::ROW;
-    const size_t row = (size_t)blockIdx.x * G::WZ + w;
+    const int w0 = threadIdx.x / G::TPF, t0 = threadIdx.x % G::TPF;
+    const size_t row = (size_t)blockIdx.x * G::WZ + w0;
     V a[G::R];
     if (kind == SRC_T) {
         const V* xr = reinterpret_cast<const V*>((const T*)a_src + row * N);
 #pragma unroll
-        for (int e = 0; e < G::R; e++) a[e] = xr[t + G::TPF * e];
+        for (int e = 0; e < G::R; e++) a[e] = xr[t0 + G::TPF * e];
     } else {
 #pragma unroll
         for (int e = 0; e < G::R; e++) {
-            const size_t n2 = row * N + 2 * (t + G::TPF * e);
+            const size_t n2 = row * N + 2 * (t0 + G::TPF * e);
             a[e] = V{load_real<T>(kind, a_src, b_src, n2), load_real<T>(kind, a_src, b_src, n2 + 1)};
         }
     }
-    SmemRow<V> sm{srow};
-    fft_passes<V, NH, G::R, false, N>(a, t, sm, tw);
+    RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
     __syncthreads();
+    r2c_row<T, N>(a, rc, dst + row * dst_stride, hout);
+}
+
+// ------------------------------------------------------------------ pair Z
+// One (i,j) row of the product of two band-limited inverse transforms,
+// transformed forward again: c2r(A) * c2r(B) -> r2c, all along l, so the real
+// product D_a*D_b (or D_a^2 when B is NULL) never leaves the SM.  Output rows
+// keep h < hout.  Persistent and double-buffered like k_inv_z.
+template <typename T, int N>
+__global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
+    k_pair_z(const V2<T>* __restrict__ srcA, int sa, int hva, const V2<T>* __restrict__ srcB, int sb,
+             int hvb, V2<T>* __restrict__ dst, int ds, int hout, const V2<T>* __restrict__ twr_g,
+             const V2<T>* __restrict__ twpp_g)
+{
+    using G = RowGeom<T, N>;
+    using V = V2<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
+    const bool two = srcB != nullptr;
+    const int PA = G::pitch(hva), PB = two ? G::pitch(hvb) : 0;
+    V* stA = reinterpret_cast<V*>(smem_raw + G::STAGE_OFF);
+    V* stB = stA + 2 * G::WZ * PA;
+    const int ntiles = N * N / G::WZ;
+    int tile = blockIdx.x;
+    if (tile < ntiles) {
+        stage_rows<V, G::WZ, G::THREADS>(stA, PA, srcA, (size_t)tile * G::WZ, sa, hva);
+        if (two) stage_rows<V, G::WZ, G::THREADS>(stB, PB, srcB, (size_t)tile * G::WZ, sb, hvb);
+    }
+    cp_async_commit();
+    for (int st = 0; tile < ntiles; tile += gridDim.x, st ^= 1) {
+        const int next = tile + gridDim.x;
+        if (next < ntiles) {
+            stage_rows<V, G::WZ, G::THREADS>(stA + (st ^ 1) * G::WZ * PA, PA, srcA, (size_t)next * G::WZ, sa, hva);
+            if (two)
+                stage_rows<V, G::WZ, G::THREADS>(stB + (st ^ 1) * G::WZ * PB, PB, srcB, (size_t)next * G::WZ, sb,
+                                                 hvb);
+        }
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();
+        const size_t row = (size_t)tile * G::WZ + rc.w;
+        V a[G::R];
+        c2r_row<T, N>(stA + st * G::WZ * PA + rc.w * PA, hva, rc, a);
+        if (two) {
+            V b[G::R];
+            c2r_row<T, N>(stB + st * G::WZ * PB + rc.w * PB, hvb, rc, b);
 #pragma unroll
-    for (int e = 0; e < G::R; e++) sm.st(t + G::TPF * e, a[e]);
-    __syncthreads();
-    V* xo = dst + row * dst_stride;
-    const T half = (T)0.5;
-    for (int k = t; k <= NH && k < hout; k += G::TPF) {
-        const V yk = sm.ld(k & (NH - 1));
-        const V ym = cconj(sm.ld((NH - k) & (NH - 1)));
-        const V E = V{(yk.x + ym.x) * half, (yk.y + ym.y) * half};
-        const V D = csub(yk, ym);
-        const V O = V{D.y * half, -D.x * half};  // D / (2i)
-        xo[k] = cadd(E, cmul(tw[k], O));
+            for (int e = 0; e < G::R; e++) a[e] = V{a[e].x * b[e].x, a[e].y * b[e].y};
+        } else {
+#pragma unroll
+            for (int e = 0; e < G::R; e++) a[e] = V{a[e].x * a[e].x, a[e].y * a[e].y};
+        }
+        // the products sit in canonical layout as (x[2n], x[2n+1]): r2c input as is
+        r2c_row<T, N>(a, rc, dst + row * ds, hout);
+        __syncthreads();
     }
 }
 
@@ -301,28 +484,53 @@ template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, const Shell* __restrict__ shells,
-            int nshell, double* __restrict__ partials, const V2<T>* __restrict__ tw)
+            int nshell, const unsigned short* __restrict__ lut, int lut_size,
+            double* __restrict__ partials, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red[(G::THREADS + 31) / 32];
-    SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw), (int)(threadIdx.x % G::W)};
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
     const int tiles_per_row = stride / G::W;
     const int j = blockIdx.x / tiles_per_row;
     const int h = (blockIdx.x % tiles_per_row) * G::W + w;
     const bool col_ok = h < hvalid && h <= N / 2;
+    const int my = lattice_freq(j, N);
+    const int mz = h == N / 2 ? -(N / 2) : h;
+    const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT;
     V a[G::R];
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int i = t + G::TPF * e;
         a[e] = data[((size_t)i * N + j) * stride + h];
     }
-    fft_passes<V, N, G::R, false, N>(a, t, sm, tw);
-    const int my = lattice_freq(j, N);
-    const int mz = h == N / 2 ? -(N / 2) : h;
-    if (epi == SPEC_STORE || epi == SPEC_STORE_PHASE || epi == SPEC_MASK_STORE) {
+    // dot / count: the shell bits depend on indices only, so they and the
+    // field values they need are fetched before the transform
+    unsigned bits[G::R];
+    V dv[G::R];
+    if (dot) {
+#pragma unroll
+        for (int e = 0; e < G::R; e++) {
+            const int i = t + G::TPF * e;
+            const int mx = lattice_freq(i, N);
+            unsigned b = 0u;
+            if (col_ok) {
+                if (lut) {
+                    const int r2 = mx * mx + my * my + mz * mz;
+                    b = r2 < lut_size ? (unsigned)__ldg(lut + r2) : 0u;
+                } else {
+                    b = shell_bits(shells, nshell, mx, my, mz);
+                }
+            }
+            bits[e] = b;
+            dv[e] = (b && epi == SPEC_DOT) ? dk[((size_t)i * N + j) * dk_stride + h] : czero<V>();
+        }
+    }
+    const V* tw = stage_table<V>(smem_raw, tw_g, N);
+    __syncthreads();
+    SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), w};
+    fft_passes<V, N, G::R, false>(a, t, sm, tw, BlockSync{});
+    if (!dot) {
         unsigned keep = (1u << G::R) - 1u;
         if (epi == SPEC_MASK_STORE) {
             keep = 0u;
@@ -355,46 +563,59 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
         }
         return;
     }
-    // SPEC_DOT / SPEC_COUNT: per-shell accumulation in FP64
+    // per-shell FP64 sums in registers, then one fixed-order reduction for all
+    // shells at once (deterministic): warp xor-trees, per-warp rows in shared
+    // memory, one thread per shell sums the rows in warp order.
     double acc[MAX_DOT_SHELLS];
 #pragma unroll
     for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = 0.0;
-    if (col_ok) {
-        const double wgt = (double)herm_weight(h, N);
-        const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
+    const double wgt = (double)herm_weight(h, N);
+    const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
 #pragma unroll
-        for (int e = 0; e < G::R; e++) {
-            const int i = t + G::TPF * e;
-            const unsigned sel = shell_bits(shells, nshell, lattice_freq(i, N), my, mz);
-            if (sel) {
-                double val;
-                if (epi == SPEC_DOT) {
-                    const V d = dk[((size_t)i * N + j) * dk_stride + h];
-                    val = wgt * ((double)d.x * (double)a[e].x + (double)d.y * (double)a[e].y);
-                } else {
-                    val = wgt * rint((double)a[e].x * inv_n3);
-                }
+    for (int e = 0; e < G::R; e++) {
+        if (bits[e]) {
+            const double val = epi == SPEC_DOT
+                                   ? wgt * ((double)dv[e].x * (double)a[e].x + (double)dv[e].y * (double)a[e].y)
+                                   : wgt * rint((double)a[e].x * inv_n3);
 #pragma unroll
-                for (int c = 0; c < MAX_DOT_SHELLS; c++)
-                    if ((sel >> c) & 1u) acc[c] += val;
-            }
+            for (int c = 0; c < MAX_DOT_SHELLS; c++)
+                if ((bits[e] >> c) & 1u) acc[c] += val;
         }
     }
-#pragma unroll 1
-    for (int c = 0; c < nshell; c++) {
-        double v = 0.0;
+    constexpr int NW = G::THREADS / 32;
+    __shared__ double wsum[NW][MAX_DOT_SHELLS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-        for (int q = 0; q < MAX_DOT_SHELLS; q++)
-            if (q == c) v = acc[q];
-        const double s = block_sum<G::THREADS>(v, red);
-        if (threadIdx.x == 0) partials[(size_t)c * gridDim.x + blockIdx.x] = s;
+    for (int c = 0; c < MAX_DOT_SHELLS; c++) {
+        double v = acc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == c) wsum[wid][c] = v;
     }
+    __syncthreads();
+    if (threadIdx.x < nshell) {
+        double sum = 0.0;
+#pragma unroll 1
+        for (int q = 0; q < NW; q++) sum += wsum[q][threadIdx.x];
+        partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = sum;
+    }
+}
+
+// Shell bitmask per r2 value (shells of the DEFAULT / RANGE kinds).
+static __global__ void k_shell_lut(const Shell* __restrict__ shells, int ns, int size,
+                                   unsigned short* __restrict__ lut)
+{
+    const int r2 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r2 >= size) return;
+    unsigned bits = 0u;
+    for (int c = 0; c < ns; c++) bits |= (unsigned)(r2 >= shells[c].r2lo && r2 <= shells[c].r2hi) << c;
+    lut[r2] = (unsigned short)bits;
 }
 
 // ------------------------------------------------------------------ final sums
 // out[c] = sum_b partials[c*nblocks + b], fixed order (one CTA per column).
 static __global__ void k_sum_partials(const double* __restrict__ partials, int nblocks, double* out,
-                               int out_stride)
+                                      int out_stride)
 {
     __shared__ double red[32];
     const double* p = partials + (size_t)blockIdx.x * nblocks;
@@ -412,7 +633,7 @@ static __global__ void k_sum_partials(const double* __restrict__ partials, int n
 // squared corners whatever the visiting order.  Non-negative doubles order
 // like their bit patterns, so the fold is an integer atomicMin/atomicMax.
 static __global__ void k_derived_range(int n, const Shell* __restrict__ shell_p, int hmax,
-                                unsigned long long* minmax_bits)
+                                       unsigned long long* minmax_bits)
 {
     const Shell sh = *shell_p;
     const int band = min(sh.band, n / 2);

@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/ps_gpu.h"
 #include "ps_kernels.cuh"
 
@@ -36,61 +38,101 @@ template <typename K> int set_smem(K kernel, size_t bytes)
     return PS_OK;
 }
 
+// Grid of a persistent kernel: as many CTAs as fit on the device at once.
+template <typename K> int persistent_grid(K kernel, int threads, size_t smem, int work_items, int* grid)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    PS_LCK(cudaGetDevice(&dev));
+    PS_LCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    PS_LCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1) per_sm = 1;
+    *grid = std::min(work_items, per_sm * sms);
+    return PS_OK;
+}
+
+// Twiddle tables of one precision: twp = Stockham table of the pencil
+// transforms (length N), twr = of the row transforms (length N/2), twpp =
+// W_N^k for the r2c / c2r pre- and post-processing (k < N).
+template <typename T> struct Tables {
+    const V2<T>* twp;
+    const V2<T>* twr;
+    const V2<T>* twpp;
+};
+
 template <typename T, int N> struct L3 {
     using V = V2<T>;
     using PG = PencilGeom<T, N>;
     using RG = RowGeom<T, N>;
+    static int pencil_width() { return PG::W; }
+    // host copies of the tables for this N
+    static void host_tables(V* twp, V* twr)
+    {
+        stockham_table<V, N, PG::R>(twp);
+        stockham_table<V, N / 2, RG::R>(twr);
+    }
     static int inv_x(cudaStream_t st, const V* src, int ss, V* dst, int ds, int mode, const Shell* sh,
-                     int hvalid, const V* tw)
+                     int hvalid, const Tables<T>& tb)
     {
         PS_LTRY(set_smem(k_inv_x<T, N>, PG::SMEM));
         k_inv_x<T, N><<<(unsigned)(N * (ds / PG::W)), PG::THREADS, PG::SMEM, st>>>(
-            src, ss, dst, ds, mode, sh, hvalid, tw);
+            src, ss, dst, ds, mode, sh, hvalid, tb.twp);
         return PS_OK;
     }
-    static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const V* tw)
+    static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb)
     {
         const unsigned blocks = (unsigned)(N * (stride / PG::W));
         if (inv) {
             PS_LTRY(set_smem(k_pass_y<T, N, true>, PG::SMEM));
-            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, tw);
+            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, tb.twp);
         } else {
             PS_LTRY(set_smem(k_pass_y<T, N, false>, PG::SMEM));
-            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, tw);
+            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, tb.twp);
         }
         return PS_OK;
     }
     static int inv_z(cudaStream_t st, const V* src, int ss, int hvalid, T* out, const T* aux, int epi,
-                     int power, double* partials, const V* tw, int* nblocks)
+                     int power, double* partials, const Tables<T>& tb, int* nblocks)
     {
-        PS_LTRY(set_smem(k_inv_z<T, N>, RG::SMEM));
-        const unsigned blocks = (unsigned)((size_t)N * N / RG::WZ);
-        k_inv_z<T, N><<<blocks, RG::THREADS, RG::SMEM, st>>>(src, ss, hvalid, out, aux, epi,
-                                                                    power, partials, tw);
-        if (nblocks) *nblocks = (int)blocks;
+        const size_t smem = RG::smem(1, hvalid, 0);
+        PS_LTRY(set_smem(k_inv_z<T, N>, RG::smem(1, N / 2 + 1, 0)));
+        int grid = 0;
+        PS_LTRY(persistent_grid(k_inv_z<T, N>, RG::THREADS, smem, N * N / RG::WZ, &grid));
+        k_inv_z<T, N><<<grid, RG::THREADS, smem, st>>>(src, ss, hvalid, out, aux, epi, power, partials,
+                                                       tb.twr, tb.twpp);
+        if (nblocks) *nblocks = grid;
         return PS_OK;
     }
     static int fwd_z(cudaStream_t st, int kind, const void* a, const void* b, V* dst, int ds, int hout,
-                     const V* tw)
+                     const Tables<T>& tb)
     {
-        PS_LTRY(set_smem(k_fwd_z<T, N>, RG::SMEM));
+        constexpr size_t smem = RG::STAGE_OFF;
+        PS_LTRY(set_smem(k_fwd_z<T, N>, smem));
         const unsigned blocks = (unsigned)((size_t)N * N / RG::WZ);
-        k_fwd_z<T, N><<<blocks, RG::THREADS, RG::SMEM, st>>>(kind, a, b, dst, ds, hout, tw);
+        k_fwd_z<T, N><<<blocks, RG::THREADS, smem, st>>>(kind, a, b, dst, ds, hout, tb.twr, tb.twpp);
+        return PS_OK;
+    }
+    static int pair_z(cudaStream_t st, const V* a, int sa, int hva, const V* b, int sb, int hvb, V* dst,
+                      int ds, int hout, const Tables<T>& tb)
+    {
+        const size_t smem = RG::smem(b ? 2 : 1, hva, hvb);
+        PS_LTRY(set_smem(k_pair_z<T, N>, RG::smem(2, N / 2 + 1, N / 2 + 1)));
+        int grid = 0;
+        PS_LTRY(persistent_grid(k_pair_z<T, N>, RG::THREADS, smem, N * N / RG::WZ, &grid));
+        k_pair_z<T, N><<<grid, RG::THREADS, smem, st>>>(a, sa, hva, b, sb, hvb, dst, ds, hout, tb.twr, tb.twpp);
         return PS_OK;
     }
     static int fwd_x(cudaStream_t st, V* data, int stride, int hvalid, int epi, V* out, int ostride,
-                     const V* dk, int dks, const Shell* shells, int nshell, double* partials,
-                     const V* tw, int* nblocks)
+                     const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
+                     int lut_size, double* partials, const Tables<T>& tb, int* nblocks)
     {
         PS_LTRY(set_smem(k_fwd_x<T, N>, PG::SMEM));
         const unsigned blocks = (unsigned)(N * (stride / PG::W));
         k_fwd_x<T, N><<<blocks, PG::THREADS, PG::SMEM, st>>>(
-            data, stride, hvalid, epi, out, ostride, dk, dks, shells, nshell, partials, tw);
+            data, stride, hvalid, epi, out, ostride, dk, dks, shells, nshell, lut, lut_size, partials, tb.twp);
         if (nblocks) *nblocks = (int)blocks;
         return PS_OK;
     }
 };
-
 
 #define PS_INSTANTIATE_L3(T)          \
     template struct L3<T, 16>;        \

@@ -81,7 +81,7 @@ int run_noalloc(cudaStream_t st, unsigned char* base, double L, const float* fie
 {
     using V32 = float2;
     using V64 = double2;
-    constexpr int W32 = PencilWidth<float>::value, W64 = PencilWidth<double>::value;
+    constexpr int W32 = PencilGeom<float, N>::W, W64 = PencilGeom<double, N>::W;
     constexpr int S32 = (N / 2 + 1 + W32 - 1) / W32 * W32;
     constexpr int S64 = (N / 2 + 1 + W64 - 1) / W64 * W64;
     size_t off = 0;
@@ -95,6 +95,12 @@ int run_noalloc(cudaStream_t st, unsigned char* base, double L, const float* fie
     V64* work64 = (V64*)carve(sizeof(V64) * (size_t)N * N * S64);
     V32* tw32 = (V32*)carve(sizeof(V32) * N);
     V64* tw64 = (V64*)carve(sizeof(V64) * N);
+    V32* twp32 = (V32*)carve(sizeof(V32) * N);
+    V32* twr32 = (V32*)carve(sizeof(V32) * N / 2);
+    V64* twp64 = (V64*)carve(sizeof(V64) * N);
+    V64* twr64 = (V64*)carve(sizeof(V64) * N / 2);
+    const Tables<float> tb32{twp32, twr32, tw32};
+    const Tables<double> tb64{twp64, twr64, tw64};
     double* partials = (double*)carve(sizeof(double) * (size_t)N * N);
     double* sums = (double*)carve(sizeof(double) * 2 * PS_NOALLOC_MAX_SHELLS);
     double* out = (double*)carve(sizeof(double) * 2 * PS_NOALLOC_MAX_SHELLS);
@@ -112,27 +118,35 @@ int run_noalloc(cudaStream_t st, unsigned char* base, double L, const float* fie
     }
     static thread_local Shell hs[PS_NOALLOC_MAX_SHELLS];
     for (int s = 0; s < ns; s++) hs[s] = host_shell(SHELL_DEFAULT, k[s], 0.0, 0.0, bw, L, N);
+    V32 hp32[N], hr32[N / 2];
+    V64 hp64[N], hr64[N / 2];
+    L3<float, N>::host_tables(hp32, hr32);
+    L3<double, N>::host_tables(hp64, hr64);
     PS_LCK(cudaMemcpyAsync(tw32, h32, sizeof(h32), cudaMemcpyHostToDevice, st));
     PS_LCK(cudaMemcpyAsync(tw64, h64, sizeof(h64), cudaMemcpyHostToDevice, st));
+    PS_LCK(cudaMemcpyAsync(twp32, hp32, sizeof(hp32), cudaMemcpyHostToDevice, st));
+    PS_LCK(cudaMemcpyAsync(twr32, hr32, sizeof(hr32), cudaMemcpyHostToDevice, st));
+    PS_LCK(cudaMemcpyAsync(twp64, hp64, sizeof(hp64), cudaMemcpyHostToDevice, st));
+    PS_LCK(cudaMemcpyAsync(twr64, hr64, sizeof(hr64), cudaMemcpyHostToDevice, st));
     PS_LCK(cudaMemcpyAsync(shells, hs, sizeof(Shell) * ns, cudaMemcpyHostToDevice, st));
 
     // forward transform of the field (get_FT_field + optional phase normalisation)
-    PS_LTRY((L3<float, N>::fwd_z(st, SRC_F32, field, nullptr, spec32, S32, N / 2 + 1, tw32)));
-    PS_LTRY((L3<float, N>::pass_y(st, spec32, S32, false, tw32)));
+    PS_LTRY((L3<float, N>::fwd_z(st, SRC_F32, field, nullptr, spec32, S32, N / 2 + 1, tb32)));
+    PS_LTRY((L3<float, N>::pass_y(st, spec32, S32, false, tb32)));
     PS_LTRY((L3<float, N>::fwd_x(st, spec32, S32, N / 2 + 1, phase == 1 ? SPEC_STORE_PHASE : SPEC_STORE,
-                                 spec32, S32, nullptr, 0, nullptr, 0, nullptr, tw32, nullptr)));
+                                 spec32, S32, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, tb32, nullptr)));
     // per shell: sum_x D^2 (FP32 transform, FP64 sum) and sum_x I^2 (FP64)
     for (int s = 0; s < ns; s++) {
         const int hb = (hs[s].band < N / 2 ? hs[s].band : N / 2) + 1;
         const int Sd = (hb + W32 - 1) / W32 * W32, Si = (hb + W64 - 1) / W64 * W64;
         int nb = 0;
-        PS_LTRY((L3<float, N>::inv_x(st, spec32, S32, work32, Sd, LOAD_MASKED, shells + s, N / 2 + 1, tw32)));
-        PS_LTRY((L3<float, N>::pass_y(st, work32, Sd, true, tw32)));
-        PS_LTRY((L3<float, N>::inv_z(st, work32, Sd, hb, nullptr, nullptr, EPI_REDUCE, 2, partials, tw32, &nb)));
+        PS_LTRY((L3<float, N>::inv_x(st, spec32, S32, work32, Sd, LOAD_MASKED, shells + s, N / 2 + 1, tb32)));
+        PS_LTRY((L3<float, N>::pass_y(st, work32, Sd, true, tb32)));
+        PS_LTRY((L3<float, N>::inv_z(st, work32, Sd, hb, nullptr, nullptr, EPI_REDUCE, 2, partials, tb32, &nb)));
         k_sum_partials<<<1, 1024, 0, st>>>(partials, nb, sums + s, 1);
-        PS_LTRY((L3<double, N>::inv_x(st, nullptr, S64, work64, Si, LOAD_UNIT, shells + s, N / 2 + 1, tw64)));
-        PS_LTRY((L3<double, N>::pass_y(st, work64, Si, true, tw64)));
-        PS_LTRY((L3<double, N>::inv_z(st, work64, Si, hb, nullptr, nullptr, EPI_REDUCE, 2, partials, tw64, &nb)));
+        PS_LTRY((L3<double, N>::inv_x(st, nullptr, S64, work64, Si, LOAD_UNIT, shells + s, N / 2 + 1, tb64)));
+        PS_LTRY((L3<double, N>::pass_y(st, work64, Si, true, tb64)));
+        PS_LTRY((L3<double, N>::inv_z(st, work64, Si, hb, nullptr, nullptr, EPI_REDUCE, 2, partials, tb64, &nb)));
         k_sum_partials<<<1, 1024, 0, st>>>(partials, nb, sums + ns + s, 1);
     }
     const double n3 = (double)N * (double)N * (double)N;
