@@ -1,0 +1,43 @@
+"""torch.autograd binding of the estimator (test / analysis helper).
+
+``polyspectrum(field, ctx, cfg, method)`` returns B of one configuration as a
+0-d float64 tensor; its backward calls ps_gpu_grad, which evaluates
+dB/d(delta) = V^(n-1) N^(-3n) / sum_I * sum_i IFFT[F_i FFT[prod_{j!=i} D_j]]
+on the GPU.  The field is the real input grid (what get_FT_field transforms,
+DENS slot, no phase normalisation).
+"""
+from __future__ import annotations
+
+import torch
+
+from . import PS_FIELD_DENS, PS_FP64_PLAIN, Context
+
+
+class _Polyspectrum(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, field: torch.Tensor, ctx: Context, cfg, method: int):
+        f = field.detach().contiguous()
+        ctx.get_FT_field(PS_FIELD_DENS, f, use_only_phase=0)
+        B, _, _, _ = ctx.batch([cfg], method)
+        fctx.ctx = ctx
+        fctx.cfg = cfg
+        fctx.method = method
+        fctx.save_for_backward(f)
+        return torch.tensor(float(B[0]), dtype=torch.float64, device=field.device)
+
+    @staticmethod
+    def backward(fctx, gout: torch.Tensor):
+        (f,) = fctx.saved_tensors
+        ctx, cfg = fctx.ctx, fctx.cfg
+        ctx.get_FT_field(PS_FIELD_DENS, f, use_only_phase=0)  # the field this B was taken on
+        g = torch.empty_like(f)
+        n = cfg.n
+        ctx.grad(n, [cfg.k[i] for i in range(n)], [cfg.kmin[i] for i in range(n)],
+                 [cfg.kmax[i] for i in range(n)], cfg.kbinwidth, cfg.kbinningCase,
+                 method=fctx.method, out=g)
+        return gout.to(g.dtype) * g, None, None, None
+
+
+def polyspectrum(field: torch.Tensor, ctx: Context, cfg, method: int = PS_FP64_PLAIN) -> torch.Tensor:
+    """B of configuration `cfg` (a ps_cfg) on `field`, differentiable in `field`."""
+    return _Polyspectrum.apply(field, ctx, cfg, method)

@@ -75,6 +75,7 @@ template <typename T> struct PrecBufs {
     V2<T>* work = nullptr;  // work spectrum (band-limited strides <= S)
     V2<T>* work2 = nullptr; // second and third work spectra (pair groups; allocated on use)
     V2<T>* work3 = nullptr;
+    V2<T>* hacc = nullptr;  // adjoint spectrum accumulator (allocated on use)
     T* ra = nullptr;        // real grids
     T* rb = nullptr;
     int S = 0;
@@ -193,6 +194,7 @@ template <typename T> void free_prec(PrecBufs<T>& b)
     cudaFree(b.work);
     cudaFree(b.work2);
     cudaFree(b.work3);
+    cudaFree(b.hacc);
     cudaFree(b.ra);
     cudaFree(b.rb);
     b = PrecBufs<T>();
@@ -277,11 +279,11 @@ namespace {
 // ---------------------------------------------------------------- profiling
 enum KernelFamily {
     KF_FWD_Z = 0, KF_PASS_Y, KF_FWD_X_STORE, KF_FWD_X_DOT, KF_INV_X, KF_INV_Z, KF_SUM, KF_DERIVED,
-    KF_FINAL, KF_PAIR_Z, KF_LUT, KF_COUNT
+    KF_FINAL, KF_PAIR_Z, KF_LUT, KF_GRAD, KF_COUNT
 };
 const char* const kFamilyName[KF_COUNT] = {"fwd_z_r2c", "pass_y", "fwd_x_store", "fwd_x_dot",
                                            "inv_x_masked", "inv_z_c2r", "sum_partials",
-                                           "derived_range", "finalize", "pair_z", "shell_lut"};
+                                           "derived_range", "finalize", "pair_z", "shell_lut", "adjoint"};
 
 int prof_fold(ps_gpu_ctx* c)
 {
@@ -942,6 +944,107 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
     return PS_OK;
 }
 
+// =========================================================================
+// adjoint: dB/d(delta) = c/sumI * c2r( sum_i F_i * FFT[prod_{j != i} D_j] )
+// =========================================================================
+template <typename T>
+int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale, void* out, int out_is_double,
+              int out_mem)
+{
+    PrecBufs<T>& B = bufs<T>(c);
+    const int N = c->N;
+    const size_t nspec = (size_t)N * N * B.S;
+    const size_t n3 = (size_t)N * N * N;
+    PS_TRY(ensure_pair_bufs(c, B));
+    PS_TRY(alloc_dev(&B.hacc, nspec));
+    PS_TRY(ensure_shells(c, PS_MAX_LEGS));
+    PS_CK(cudaMemcpyAsync(c->dshells, legs.data(), sizeof(Shell) * n, cudaMemcpyHostToDevice, c->stream));
+    PS_CK(cudaMemsetAsync(B.hacc, 0, sizeof(V2<T>) * nspec, c->stream));
+    int hb = 1;
+    for (int l = 0; l < n; l++) hb = std::max(hb, std::min(legs[l].band, N / 2) + 1);
+    if (n == 2) {
+        Prof pf(c);
+        k_grad_pair2<T><<<148 * 8, 256, 0, c->stream>>>(N, B.spec, B.S, c->dshells, B.hacc, B.S, hb);
+        pf.end(KF_GRAD, 2.0 * N * N * hb * sizeof(V2<T>));
+    } else {
+        // leg i: FFT of the product of the other two legs, masked by F_i;
+        // identical (mask, pair) terms are folded into one with a weight
+        std::vector<std::pair<std::vector<int>, int>> terms;
+        for (int i = 0; i < 3; i++) {
+            std::vector<int> key = {i, (i + 1) % 3, (i + 2) % 3};
+            if (key[1] > key[2]) std::swap(key[1], key[2]);
+            bool found = false;
+            for (auto& tm : terms) {
+                const auto& k0 = tm.first;
+                if (same_shell(legs[k0[0]], legs[key[0]]) &&
+                    ((same_shell(legs[k0[1]], legs[key[1]]) && same_shell(legs[k0[2]], legs[key[2]])) ||
+                     (same_shell(legs[k0[1]], legs[key[2]]) && same_shell(legs[k0[2]], legs[key[1]])))) {
+                    tm.second++;
+                    found = true;
+                    break;
+                }
+            }
+            if (!found) terms.push_back({key, 1});
+        }
+        for (const auto& tm : terms) {
+            const int li = tm.first[0], la = tm.first[1], lb = tm.first[2];
+            const bool same = same_shell(legs[la], legs[lb]);
+            int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
+            PS_TRY(c2r_xy<T>(c, LOAD_MASKED, c->dshells + la, legs[la].band, B.work, &Sa, &ha));
+            if (!same) PS_TRY(c2r_xy<T>(c, LOAD_MASKED, c->dshells + lb, legs[lb].band, B.work2, &Sb, &hbb));
+            const int hout = std::min(legs[li].band, N / 2) + 1;
+            PS_TRY(pair_spectrum<T>(c, B.work, Sa, ha, same ? nullptr : B.work2, Sb, hbb, hout, &S));
+            Prof pf(c);
+            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.work3, S, hout, SPEC_MASK_ADD, B.hacc, B.S, nullptr,
+                                                    0, c->dshells + li, 1, nullptr, 0, nullptr, B.tables(),
+                                                    nullptr, (double)tm.second))));
+            pf.end(KF_GRAD, 3.0 * N * N * S * sizeof(V2<T>));
+        }
+    }
+    // inverse transform of the accumulated spectrum into B.ra, then scale
+    const int S = round_up(hb, pw<T>(N));
+    int nb = 0;
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.hacc, B.S, B.work, S, LOAD_PLAIN, nullptr, hb, B.tables()))));
+        pf.end(KF_INV_X, 2.0 * N * N * S * sizeof(V2<T>));
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, true, B.tables()))));
+        pf.end(KF_PASS_Y, 2.0 * N * N * S * sizeof(V2<T>));
+    }
+    {
+        Prof pf(c);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_z(c->stream, B.work, S, hb, B.ra, nullptr, EPI_STORE, 1, nullptr,
+                                                B.tables(), &nb))));
+        pf.end(KF_INV_Z, (double)N * N * hb * sizeof(V2<T>) + (double)n3 * sizeof(T));
+    }
+    void* dst = out;
+    void* stage = nullptr;
+    const size_t out_bytes = n3 * (out_is_double ? 8 : 4);
+    if (out_mem == PS_MEM_HOST) {
+        PS_TRY(alloc_dev((unsigned char**)&stage, out_bytes));
+        dst = stage;
+    }
+    {
+        Prof pf(c);
+        if (out_is_double)
+            k_scale_out<T, double><<<148 * 8, 256, 0, c->stream>>>(B.ra, (double*)dst, n3, scale);
+        else
+            k_scale_out<T, float><<<148 * 8, 256, 0, c->stream>>>(B.ra, (float*)dst, n3, scale);
+        pf.end(KF_GRAD, (double)n3 * (sizeof(T) + (out_is_double ? 8 : 4)));
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && stage) {
+        e = cudaMemcpyAsync(out, stage, out_bytes, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(stage);
+    PS_CK(e);
+    return PS_OK;
+}
+
 int timed_begin(ps_gpu_ctx* c)
 {
     c->launches = 0;
@@ -1134,9 +1237,44 @@ int ps_gpu_grad(ps_gpu_ctx* c, int method, int n, const double* k, const double*
                 const double* kmax, double kbinwidth, int kbinningCase, void* out, int out_is_double,
                 int out_mem)
 {
-    (void)c; (void)method; (void)n; (void)k; (void)kmin; (void)kmax; (void)kbinwidth;
-    (void)kbinningCase; (void)out; (void)out_is_double; (void)out_mem;
-    return fail(PS_ERR_UNSUPPORTED, "ps_gpu_grad: not built yet");
+    g_err[0] = 0;
+    if (!c || !k || !kmin || !kmax || !out) return fail(PS_ERR_ARG, "NULL argument");
+    if (!c->field_set) return fail(PS_ERR_ARG, "no field loaded (ps_gpu_set_field)");
+    if (method != PS_FP64_PLAIN && method != PS_FP32_BATCHED) return fail(PS_ERR_ARG, "method %d", method);
+    if (!(c->methods & method)) return fail(PS_ERR_ARG, "method %d not enabled for this context", method);
+    if (out_mem != PS_MEM_HOST && out_mem != PS_MEM_DEVICE) return fail(PS_ERR_ARG, "out_mem=%d", out_mem);
+    if (n != 2 && n != 3)
+        return fail(PS_ERR_UNSUPPORTED, "ps_gpu_grad: n=%d (the reference's configurations have n = 2 or 3)", n);
+    if (c->use_only_phase == 1)
+        return fail(PS_ERR_UNSUPPORTED, "ps_gpu_grad: the field was loaded phase-only; the gradient is defined "
+                                        "for use_only_phase = 0");
+    PS_CK(cudaSetDevice(c->device));
+    ps_cfg g;
+    memset(&g, 0, sizeof(g));
+    g.n = n;
+    g.kbinningCase = kbinningCase;
+    g.kbinwidth = kbinwidth;
+    for (int l = 0; l < n; l++) {
+        g.k[l] = k[l];
+        g.kmin[l] = kmin[l];
+        g.kmax[l] = kmax[l];
+    }
+    // B and the polygon count of the configuration (sum I = N^3 * Npoly)
+    double Bv = 0.0, Np = 0.0;
+    {
+        ps_cfg g2 = g;
+        int rc = method == PS_FP64_PLAIN ? plain_batch(c, 1, &g2, &Bv, &Np) : batched(c, 1, &g2, &Bv, &Np);
+        if (rc != PS_OK) return rc;
+    }
+    PS_TRY(timed_begin(c));
+    std::vector<std::vector<Shell>> legs;
+    PS_TRY(resolve_legs(c, 1, &g, legs));
+    const double n3 = (double)c->N * (double)c->N * (double)c->N;
+    const double scale = norm_coef(c->L, c->N, n) / (Np * n3);
+    int rc = method == PS_FP64_PLAIN ? grad_impl<double>(c, n, legs[0], scale, out, out_is_double, out_mem)
+                                     : grad_impl<float>(c, n, legs[0], scale, out, out_is_double, out_mem);
+    if (rc != PS_OK) return rc;
+    return timed_end(c);
 }
 
 int ps_make_configs(const ps_run_params* p, ps_cfg* cfgs, int max_cfg, double* k_out, double* theta_out)

@@ -477,14 +477,14 @@ enum SpecEpi : int {
     SPEC_STORE_PHASE = 1,  // out = X / |X|  (utils_fftw.c:78-93)
     SPEC_DOT = 2,          // per shell c: sum_m w(h) F_c(m) Re(dk(m) conj(X(m)))
     SPEC_COUNT = 3,        // per shell c: sum_m w(h) F_c(m) rint(Re X(m) / N^3)
-    SPEC_MASK_STORE = 4    // out = F(m) X(m)
+    SPEC_MASK_ADD = 4      // out += weight * F(m) X(m) where F selects (adjoint)
 };
 
 template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, const Shell* __restrict__ shells,
-            int nshell, const unsigned short* __restrict__ lut, int lut_size,
+            int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight,
             double* __restrict__ partials, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     fft_passes<V, N, G::R, false>(a, t, sm, tw, BlockSync{});
     if (!dot) {
         unsigned keep = (1u << G::R) - 1u;
-        if (epi == SPEC_MASK_STORE) {
+        if (epi == SPEC_MASK_ADD) {
             keep = 0u;
             const Shell sh = shells[0];
             if (col_ok) {
@@ -556,8 +556,12 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
                     const float m = hypotf(v.x, v.y);
                     v = V{v.x / m, v.y / m};
                 }
-            } else if (!((keep >> e) & 1u)) {
-                v = czero<V>();
+            } else if (epi == SPEC_MASK_ADD) {
+                if (!((keep >> e) & 1u)) continue;
+                V* o = out + ((size_t)i * N + j) * out_stride + h;
+                const V prev = *o;
+                *o = V{prev.x + (T)weight * v.x, prev.y + (T)weight * v.y};
+                continue;
             }
             out[((size_t)i * N + j) * out_stride + h] = v;
         }
@@ -610,6 +614,39 @@ static __global__ void k_shell_lut(const Shell* __restrict__ shells, int ns, int
     unsigned bits = 0u;
     for (int c = 0; c < ns; c++) bits |= (unsigned)(r2 >= shells[c].r2lo && r2 <= shells[c].r2hi) << c;
     lut[r2] = (unsigned short)bits;
+}
+
+// ------------------------------------------------------------------ adjoint helpers
+// n = 2: dB/d(delta) needs L_a D_b + L_b D_a = IFFT[F_a FFT[D_b] + F_b FFT[D_a]]
+// with FFT[D] = N^3 F dk (the inverse transform is unnormalised), i.e.
+// IFFT[2 N^3 F_a F_b dk]; this writes that spectrum on the band h < hb (stride S).
+template <typename T>
+__global__ void k_grad_pair2(int n, const V2<T>* __restrict__ dk, int dks, const Shell* __restrict__ shells,
+                             V2<T>* __restrict__ hacc, int S, int hb)
+{
+    const size_t total = (size_t)n * n * hb;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const int h = (int)(q % hb);
+        const size_t r = q / hb;
+        const int j = (int)(r % n), i = (int)(r / n);
+        const int mx = lattice_freq(i, n), my = lattice_freq(j, n), mz = h == n / 2 ? -(n / 2) : h;
+        V2<T> v = czero<V2<T>>();
+        if (h <= n / 2 && in_band(shells[0], mx, my, mz) && shell_bit(shells[0], mx, my, mz) &&
+            in_band(shells[1], mx, my, mz) && shell_bit(shells[1], mx, my, mz)) {
+            const V2<T> d = dk[r * dks + h];
+            const T f = (T)(2.0 * (double)n * (double)n * (double)n);
+            v = V2<T>{f * d.x, f * d.y};
+        }
+        hacc[r * S + h] = v;
+    }
+}
+
+// out[x] = scale * in[x], converted to the output type.
+template <typename T, typename O>
+__global__ void k_scale_out(const T* __restrict__ in, O* __restrict__ out, size_t count, double scale)
+{
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < count; q += (size_t)gridDim.x * blockDim.x)
+        out[q] = (O)(scale * (double)in[q]);
 }
 
 // ------------------------------------------------------------------ final sums

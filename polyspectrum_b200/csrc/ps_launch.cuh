@@ -123,12 +123,13 @@ template <typename T, int N> struct L3 {
     }
     static int fwd_x(cudaStream_t st, V* data, int stride, int hvalid, int epi, V* out, int ostride,
                      const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
-                     int lut_size, double* partials, const Tables<T>& tb, int* nblocks)
+                     int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0)
     {
         PS_LTRY(set_smem(k_fwd_x<T, N>, PG::SMEM));
         const unsigned blocks = (unsigned)(N * (stride / PG::W));
         k_fwd_x<T, N><<<blocks, PG::THREADS, PG::SMEM, st>>>(
-            data, stride, hvalid, epi, out, ostride, dk, dks, shells, nshell, lut, lut_size, partials, tb.twp);
+            data, stride, hvalid, epi, out, ostride, dk, dks, shells, nshell, lut, lut_size, weight, partials,
+            tb.twp);
         if (nblocks) *nblocks = (int)blocks;
         return PS_OK;
     }
