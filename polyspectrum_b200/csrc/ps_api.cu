@@ -101,6 +101,8 @@ struct ps_gpu_ctx {
     size_t dminmax_cap = 0;
     unsigned short* dlut = nullptr;  // r2 -> shell bitmask
     size_t dlut_cap = 0;
+    int* didx = nullptr;  // scatter indices
+    size_t didx_cap = 0;
     void* stage[2] = {nullptr, nullptr};
     size_t stage_bytes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -248,6 +250,16 @@ int ensure_lut(ps_gpu_ctx* c, size_t n)
     c->dlut_cap = n;
     return PS_OK;
 }
+int ensure_idx(ps_gpu_ctx* c, size_t n)
+{
+    if (n <= c->didx_cap) return PS_OK;
+    cudaFree(c->didx);
+    c->didx = nullptr;
+    c->didx_cap = 0;
+    PS_TRY(alloc_dev(&c->didx, n));
+    c->didx_cap = n;
+    return PS_OK;
+}
 int ensure_minmax(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->dminmax_cap) return PS_OK;
@@ -279,11 +291,12 @@ namespace {
 // ---------------------------------------------------------------- profiling
 enum KernelFamily {
     KF_FWD_Z = 0, KF_PASS_Y, KF_FWD_X_STORE, KF_FWD_X_DOT, KF_INV_X, KF_INV_Z, KF_SUM, KF_DERIVED,
-    KF_FINAL, KF_PAIR_Z, KF_LUT, KF_GRAD, KF_COUNT
+    KF_FINAL, KF_PAIR_Z, KF_LUT, KF_GRAD, KF_PAIR2, KF_COUNT
 };
 const char* const kFamilyName[KF_COUNT] = {"fwd_z_r2c", "pass_y", "fwd_x_store", "fwd_x_dot",
                                            "inv_x_masked", "inv_z_c2r", "sum_partials",
-                                           "derived_range", "finalize", "pair_z", "shell_lut", "adjoint"};
+                                           "derived_range", "finalize", "pair_z", "shell_lut", "adjoint",
+                                           "pair2_parseval"};
 
 int prof_fold(ps_gpu_ctx* c)
 {
@@ -377,7 +390,7 @@ int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, co
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
-    const bool reduce = epi == EPI_MUL_REDUCE || epi == EPI_REDUCE;
+    const bool reduce = epi >= EPI_MUL_REDUCE;
     if (reduce) PS_TRY(ensure_partials(c, (size_t)N * N));
     int S = 0, hb = 0, nb = 0;
     PS_TRY(c2r_xy<T>(c, mode, dshell, band, B.work, &S, &hb));
@@ -717,14 +730,14 @@ double norm_coef(double L, int N, int n)
 // =========================================================================
 // method 1: plain FP64, reference dataflow
 // =========================================================================
-int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
+int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, double* kappa)
 {
     if (!c->d.have_spec) return fail(PS_ERR_ARG, "FP64 spectrum not available (methods mask)");
     std::vector<std::vector<Shell>> legs;
     const int N = c->N;
     PS_TRY(ensure_sums(c, 4 * (size_t)nconf + 8));
     PS_TRY(ensure_shells(c, PS_MAX_LEGS));
-    std::vector<double> coef(nconf);
+    std::vector<double> coef(nconf), habs(nconf, 0.0);
     for (int q = 0; q < nconf; q++) {
         PS_TRY(resolve_legs(c, 1, cfgs + q, legs));
         const int n = cfgs[q].n;
@@ -739,6 +752,12 @@ int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
                 const int epi = l == 0 ? EPI_STORE : (l < n - 1 ? EPI_MUL_STORE : EPI_MUL_REDUCE);
                 PS_TRY(c2r_shell<double>(c, mode, c->dshells + l, legs[0][l].band, prod, prod, epi, 1,
                                          pass == 0 ? sD : sI));
+                if (kappa && pass == 0 && l == n - 1) {  // sum |prod D| for the condition number
+                    double* sA = c->dsums + 3 * nconf + q;
+                    PS_TRY(c2r_shell<double>(c, mode, c->dshells + l, legs[0][l].band, prod, prod,
+                                             EPI_MUL_REDUCE_ABS, 1, sA));
+                    PS_CK(cudaMemcpyAsync(&habs[q], sA, 8, cudaMemcpyDeviceToHost, c->stream));
+                }
             }
         }
         coef[q] = norm_coef(c->L, N, n);
@@ -757,8 +776,11 @@ int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
         pf.end(KF_FINAL, 0.0);
     }
     std::vector<double> h(2 * nconf);
+    std::vector<double> hD(nconf);
     cudaError_t e1 = cudaMemcpyAsync(h.data(), dout, sizeof(double) * 2 * nconf, cudaMemcpyDeviceToHost,
                                      c->stream);
+    if (e1 == cudaSuccess && kappa)
+        e1 = cudaMemcpyAsync(hD.data(), c->dsums, sizeof(double) * nconf, cudaMemcpyDeviceToHost, c->stream);
     cudaError_t e2 = cudaStreamSynchronize(c->stream);
     cudaFree(dout);
     PS_CK(e1);
@@ -766,6 +788,7 @@ int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
     for (int q = 0; q < nconf; q++) {
         B[q] = h[2 * q];
         Np[q] = h[2 * q + 1];
+        if (kappa) kappa[q] = habs[q] / fabs(hD[q]);
     }
     return PS_OK;
 }
@@ -779,7 +802,77 @@ struct Group {  // n=3 configurations sharing the leg pair (a, b)
     std::vector<int> third;  // shell id of each configuration's remaining leg
 };
 
-int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
+// dst[idx[q]] = src[q], q < count (idx uploaded from the host).
+int scatter(ps_gpu_ctx* c, const double* src, const std::vector<int>& idx, double* dst)
+{
+    if (idx.empty()) return PS_OK;
+    PS_TRY(ensure_idx(c, idx.size()));
+    PS_CK(cudaMemcpyAsync(c->didx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, c->stream));
+    Prof pf(c);
+    k_scatter<<<((int)idx.size() + 127) / 128, 128, 0, c->stream>>>(src, c->didx, (int)idx.size(), dst);
+    pf.end(KF_SUM, 16.0 * idx.size());
+    return PS_OK;
+}
+
+// n = 2 configurations: sum_x D_a D_b = N^3 sum_m F_a F_b |dk|^2 and the exact
+// count of shared modes, one k-space pass per MAX_DOT_SHELLS configurations.
+int pair2_sums(ps_gpu_ctx* c, const std::vector<int>& qs, const std::vector<std::vector<int>>& lid,
+               const std::vector<Shell>& uniq, double* sumD, double* sumI, double* scratch)
+{
+    const int N = c->N;
+    for (size_t q0 = 0; q0 < qs.size(); q0 += MAX_DOT_SHELLS) {
+        const int cnt = (int)std::min<size_t>(MAX_DOT_SHELLS, qs.size() - q0);
+        std::vector<Shell> pairs;  // legs of each configuration, then the interval pseudo-shells
+        bool lut_ok = true;
+        int band = 0, lut_size = 0;
+        for (int x = 0; x < cnt; x++) {
+            const Shell& sa = uniq[lid[qs[q0 + x]][0]];
+            const Shell& sb = uniq[lid[qs[q0 + x]][1]];
+            pairs.push_back(sa);
+            pairs.push_back(sb);
+            band = std::max(band, std::min(sa.band, sb.band));
+            if (sa.kind > SHELL_RANGE || sb.kind > SHELL_RANGE) lut_ok = false;
+        }
+        for (int x = 0; x < cnt && lut_ok; x++) {
+            Shell iv = pairs[2 * x];
+            iv.r2lo = std::max(pairs[2 * x].r2lo, pairs[2 * x + 1].r2lo);
+            iv.r2hi = std::min(pairs[2 * x].r2hi, pairs[2 * x + 1].r2hi);
+            lut_size = std::max(lut_size, iv.r2hi + 1);
+            pairs.push_back(iv);
+        }
+        PS_TRY(ensure_shells(c, pairs.size()));
+        PS_CK(cudaMemcpyAsync(c->dshells, pairs.data(), sizeof(Shell) * pairs.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+        const unsigned short* lut = nullptr;
+        if (lut_ok) {
+            PS_TRY(ensure_lut(c, (size_t)std::max(lut_size, 1)));
+            Prof pf(c);
+            if (lut_size > 0)
+                k_shell_lut<<<(lut_size + 255) / 256, 256, 0, c->stream>>>(c->dshells + 2 * cnt, cnt, lut_size,
+                                                                           c->dlut);
+            pf.end(KF_LUT, 2.0 * lut_size);
+            lut = c->dlut;
+        }
+        const int b = std::min(band, N / 2);
+        const long long modes = (long long)(2 * b + 1) * (2 * b + 1) * (b + 1);
+        const int blocks = (int)std::max<long long>(1, std::min<long long>((modes + 255) / 256, 148 * 8));
+        PS_TRY(ensure_partials(c, (size_t)blocks * 2 * MAX_DOT_SHELLS));
+        {
+            Prof pf(c);
+            k_pair2_sums<float><<<blocks, 256, 0, c->stream>>>(N, c->f.spec, c->f.S, lut, lut_size, c->dshells, cnt,
+                                                               b, c->partials);
+            pf.end(KF_PAIR2, (double)modes * sizeof(V2<float>));
+        }
+        PS_TRY(sum_partials(c, blocks, 2 * MAX_DOT_SHELLS, scratch, 1));
+        std::vector<int> idx(qs.begin() + q0, qs.begin() + q0 + cnt);
+        PS_TRY(scatter(c, scratch, idx, sumD));
+        PS_TRY(scatter(c, scratch + MAX_DOT_SHELLS, idx, sumI));
+    }
+    PS_CK(cudaGetLastError());
+    return PS_OK;
+}
+
+int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, double* kappa)
 {
     if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available (methods mask)");
     const int N = c->N;
@@ -797,10 +890,10 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
             lid[q].push_back(id);
         }
     }
-    // device shell table: unique shells, then per-group third-leg lists
+    // plan: pair groups (n = 3 sharing a leg pair), n = 2 (Parseval), the rest leg by leg
     std::vector<Group> groups;
-    std::vector<int> direct;      // configurations evaluated leg by leg
-    std::vector<int> pairs2;      // n == 2 configurations (Parseval, no transform)
+    std::vector<int> direct;
+    std::vector<int> pairs2;
     {
         std::map<std::pair<int, int>, int> freq;
         for (int q = 0; q < nconf; q++)
@@ -834,7 +927,24 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
             groups[it->second].third.push_back(v[z]);
         }
     }
-    // shell table layout: [uniq][group thirds...][pairs2: (a,b) interleaved? no: we pass a,b]
+    // device scalars: sumD | sumI | coef | scratch D | scratch I | sumA (|terms|) | scratch A
+    PS_TRY(ensure_sums(c, 7 * (size_t)nconf + 4 * MAX_DOT_SHELLS + 8));
+    double* sumD = c->dsums;
+    double* sumI = sumD + nconf;  // exact polygon counts
+    double* dcoef = sumI + nconf;
+    double* gD = dcoef + nconf;
+    double* gI = gD + std::max(nconf, 2 * MAX_DOT_SHELLS);
+    double* sumA = gI + std::max(nconf, 2 * MAX_DOT_SHELLS);
+    double* gA = sumA + nconf;
+    std::vector<double> coef(nconf);
+    for (int q = 0; q < nconf; q++) coef[q] = norm_coef(c->L, N, cfgs[q].n);
+    std::vector<double> hsI_direct;
+
+    // ---- pair groups
+    if (!groups.empty()) {
+        PS_TRY(ensure_pair_bufs(c, c->f));
+        PS_TRY(ensure_pair_bufs(c, c->d));
+    }
     std::vector<Shell> table = uniq;
     std::vector<int> gofs(groups.size());
     for (size_t g = 0; g < groups.size(); g++) {
@@ -842,19 +952,8 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
         for (int s : groups[g].third) table.push_back(uniq[s]);
     }
     PS_TRY(ensure_shells(c, table.size()));
-    PS_CK(cudaMemcpyAsync(c->dshells, table.data(), sizeof(Shell) * table.size(),
-                          cudaMemcpyHostToDevice, c->stream));
-    PS_TRY(ensure_sums(c, 4 * (size_t)nconf + 8));
-    if (!groups.empty()) {
-        PS_TRY(ensure_pair_bufs(c, c->f));
-        PS_TRY(ensure_pair_bufs(c, c->d));
-    }
-    double* sumD = c->dsums;
-    double* sumI = c->dsums + nconf;  // exact counts (count mode)
-    std::vector<double> coef(nconf);
-    for (int q = 0; q < nconf; q++) coef[q] = norm_coef(c->L, N, cfgs[q].n);
-
-    // ---- shared-pair groups: Parseval over the closing legs
+    PS_CK(cudaMemcpyAsync(c->dshells, table.data(), sizeof(Shell) * table.size(), cudaMemcpyHostToDevice,
+                          c->stream));
     for (size_t g = 0; g < groups.size(); g++) {
         const Group& G = groups[g];
         const Shell& sa = uniq[G.a];
@@ -863,9 +962,6 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
         for (int s : G.third) hmax = std::max(hmax, std::min(uniq[s].band, N / 2));
         const int hout = hmax + 1;
         const int ng = (int)G.cfg.size();
-        // scratch sums for the group, then scatter
-        double* gD = c->dsums + 2 * nconf;
-        double* gI = c->dsums + 3 * nconf;
         // D part (FP32): P = D_a * D_b formed row by row and transformed back,
         // then one masked dot product with dk per closing shell
         int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
@@ -873,21 +969,28 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
         if (G.a != G.b) PS_TRY(c2r_xy<float>(c, LOAD_MASKED, c->dshells + G.b, sb.band, c->f.work2, &Sb, &hbb));
         PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout, &S));
         PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gD));
+        if (kappa)
+            PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, c->dshells + gofs[g], table.data() + gofs[g],
+                                   ng, gA));
         // I part (FP64): the same on unit shells, counts rounded per mode
         PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.work, &Sa, &ha));
         if (G.a != G.b) PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.b, sb.band, c->d.work2, &Sb, &hbb));
         PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S));
         PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gI));
-        for (int x = 0; x < ng; x++) {
-            PS_CK(cudaMemcpyAsync(sumD + G.cfg[x], gD + x, 8, cudaMemcpyDeviceToDevice, c->stream));
-            PS_CK(cudaMemcpyAsync(sumI + G.cfg[x], gI + x, 8, cudaMemcpyDeviceToDevice, c->stream));
-        }
+        PS_TRY(scatter(c, gD, G.cfg, sumD));
+        PS_TRY(scatter(c, gI, G.cfg, sumI));
+        if (kappa) PS_TRY(scatter(c, gA, G.cfg, sumA));
     }
 
-    // ---- n = 2: sum_x D_a D_b = N^3 sum_m F_a F_b |dk|^2 -> reuse the leg-by-leg path
-    for (int q : pairs2) direct.push_back(q);
+    // ---- n = 2 (all terms are |dk|^2 >= 0: condition number 1)
+    if (!pairs2.empty()) PS_TRY(pair2_sums(c, pairs2, lid, uniq, sumD, sumI, gD));
 
-    // ---- leg by leg (singletons, n = 2, n > 3): running products with powers
+    // ---- leg by leg (singletons, n > 3): running products with powers
+    if (!direct.empty()) {
+        PS_TRY(ensure_shells(c, uniq.size()));
+        PS_CK(cudaMemcpyAsync(c->dshells, uniq.data(), sizeof(Shell) * uniq.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+    }
     for (int q : direct) {
         const auto& v = lid[q];
         std::vector<std::pair<int, int>> up;  // (shell, multiplicity)
@@ -904,25 +1007,30 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
                 if (r == 1) epi = EPI_REDUCE;
                 else epi = x == 0 ? EPI_STORE : (x < r - 1 ? EPI_MUL_STORE : EPI_MUL_REDUCE);
                 const Shell& s = uniq[up[x].first];
-                if (pass == 0)
-                    PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + up[x].first, s.band, c->f.ra,
-                                            c->f.ra, epi, up[x].second, sumD + q));
-                else
-                    PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + up[x].first, s.band, c->d.ra,
-                                             c->d.ra, epi, up[x].second, sumI + q));
+                if (pass == 0) {
+                    PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + up[x].first, s.band, c->f.ra, c->f.ra, epi,
+                                            up[x].second, sumD + q));
+                    if (kappa && x == r - 1)  // |terms| of the same final sum
+                        PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + up[x].first, s.band, c->f.ra, c->f.ra,
+                                                r == 1 ? EPI_REDUCE_ABS : EPI_MUL_REDUCE_ABS, up[x].second,
+                                                sumA + q));
+                } else {
+                    PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + up[x].first, s.band, c->d.ra, c->d.ra, epi,
+                                             up[x].second, sumI + q));
+                }
             }
         }
     }
     // direct configurations hold grid sums in sumI: convert them to counts
     // (round(sumI / N^3), exact since the FP64 error is far below 1/2)
-    std::vector<double> hsD(nconf), hsI(nconf);
-    PS_CK(cudaMemcpyAsync(hsD.data(), sumD, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream));
-    PS_CK(cudaMemcpyAsync(hsI.data(), sumI, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream));
-    PS_CK(cudaStreamSynchronize(c->stream));
     const double n3 = (double)N * (double)N * (double)N;
-    for (int q : direct) hsI[q] = nearbyint(hsI[q] / n3);
-    PS_CK(cudaMemcpyAsync(sumI, hsI.data(), 8 * (size_t)nconf, cudaMemcpyHostToDevice, c->stream));
-    double* dcoef = c->dsums + 2 * nconf;
+    if (!direct.empty()) {
+        std::vector<double> hsI(nconf);
+        PS_CK(cudaMemcpyAsync(hsI.data(), sumI, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream));
+        PS_CK(cudaStreamSynchronize(c->stream));
+        for (int q : direct) hsI[q] = nearbyint(hsI[q] / n3);
+        PS_CK(cudaMemcpyAsync(sumI, hsI.data(), 8 * (size_t)nconf, cudaMemcpyHostToDevice, c->stream));
+    }
     PS_CK(cudaMemcpyAsync(dcoef, coef.data(), 8 * (size_t)nconf, cudaMemcpyHostToDevice, c->stream));
     double* dout = nullptr;
     PS_TRY(alloc_dev(&dout, 2 * (size_t)nconf));
@@ -931,8 +1039,14 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
         k_finalize<<<(nconf + 127) / 128, 128, 0, c->stream>>>(nconf, dcoef, sumD, sumI, 1.0 / n3, 1, dout);
         pf.end(KF_FINAL, 0.0);
     }
-    std::vector<double> h(2 * nconf);
+    std::vector<double> h(2 * nconf), hA, hD;
     cudaError_t e1 = cudaMemcpyAsync(h.data(), dout, 16 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream);
+    if (kappa && e1 == cudaSuccess) {
+        hA.resize(nconf);
+        hD.resize(nconf);
+        e1 = cudaMemcpyAsync(hA.data(), sumA, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream);
+        if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(hD.data(), sumD, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream);
+    }
     cudaError_t e2 = cudaStreamSynchronize(c->stream);
     cudaFree(dout);
     PS_CK(e1);
@@ -940,6 +1054,9 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np)
     for (int q = 0; q < nconf; q++) {
         B[q] = h[2 * q];
         Np[q] = h[2 * q + 1];
+    }
+    if (kappa) {
+        for (int q = 0; q < nconf; q++) kappa[q] = cfgs[q].n == 2 ? 1.0 : hA[q] / fabs(hD[q]);
     }
     return PS_OK;
 }
@@ -1200,11 +1317,9 @@ int ps_gpu_polyspectrum_batch(ps_gpu_ctx* c, int method, int nconf, ps_cfg* cfgs
     if (!(c->methods & method)) return fail(PS_ERR_ARG, "method %d not enabled for this context", method);
     PS_CK(cudaSetDevice(c->device));
     PS_TRY(timed_begin(c));
-    int rc = method == PS_FP64_PLAIN ? plain_batch(c, nconf, cfgs, B, Npoly)
-                                     : batched(c, nconf, cfgs, B, Npoly);
+    int rc = method == PS_FP64_PLAIN ? plain_batch(c, nconf, cfgs, B, Npoly, kappa)
+                                     : batched(c, nconf, cfgs, B, Npoly, kappa);
     if (rc != PS_OK) return rc;
-    if (kappa)
-        for (int q = 0; q < nconf; q++) kappa[q] = NAN;
     return timed_end(c);
 }
 
@@ -1263,7 +1378,8 @@ int ps_gpu_grad(ps_gpu_ctx* c, int method, int n, const double* k, const double*
     double Bv = 0.0, Np = 0.0;
     {
         ps_cfg g2 = g;
-        int rc = method == PS_FP64_PLAIN ? plain_batch(c, 1, &g2, &Bv, &Np) : batched(c, 1, &g2, &Bv, &Np);
+        int rc = method == PS_FP64_PLAIN ? plain_batch(c, 1, &g2, &Bv, &Np, nullptr)
+                                         : batched(c, 1, &g2, &Bv, &Np, nullptr);
         if (rc != PS_OK) return rc;
     }
     PS_TRY(timed_begin(c));
@@ -1415,6 +1531,7 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     cudaFree(c->dshells);
     cudaFree(c->dminmax);
     cudaFree(c->dlut);
+    cudaFree(c->didx);
     cudaFree(c->stage[0]);
     cudaFree(c->stage[1]);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);

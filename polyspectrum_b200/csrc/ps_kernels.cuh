@@ -290,7 +290,9 @@ enum RealEpi : int {
     EPI_STORE = 0,      // out = x^p
     EPI_MUL_STORE = 1,  // out = x^p * aux   (aux may alias out)
     EPI_MUL_REDUCE = 2, // sum x^p * aux
-    EPI_REDUCE = 3      // sum x^p
+    EPI_REDUCE = 3,     // sum x^p
+    EPI_MUL_REDUCE_ABS = 4,  // sum |x^p * aux|  (condition numbers)
+    EPI_REDUCE_ABS = 5       // sum |x^p|
 };
 
 template <typename T> __device__ __forceinline__ T ipow(T x, int p)
@@ -345,13 +347,18 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
             } else if (epi == EPI_MUL_REDUCE) {
                 const V q = *reinterpret_cast<const V*>(arow + n2);
                 acc += (double)x0 * (double)q.x + (double)x1 * (double)q.y;
+            } else if (epi == EPI_MUL_REDUCE_ABS) {
+                const V q = *reinterpret_cast<const V*>(arow + n2);
+                acc += fabs((double)x0 * (double)q.x) + fabs((double)x1 * (double)q.y);
+            } else if (epi == EPI_REDUCE_ABS) {
+                acc += fabs((double)x0) + fabs((double)x1);
             } else {
                 acc += (double)x0 + (double)x1;
             }
         }
         __syncthreads();  // stage st is refilled two tiles later
     }
-    if (epi == EPI_MUL_REDUCE || epi == EPI_REDUCE) {
+    if (epi >= EPI_MUL_REDUCE) {
         const double s = block_sum<G::THREADS>(acc, red);
         if (threadIdx.x == 0) partials[blockIdx.x] = s;
     }
@@ -477,7 +484,8 @@ enum SpecEpi : int {
     SPEC_STORE_PHASE = 1,  // out = X / |X|  (utils_fftw.c:78-93)
     SPEC_DOT = 2,          // per shell c: sum_m w(h) F_c(m) Re(dk(m) conj(X(m)))
     SPEC_COUNT = 3,        // per shell c: sum_m w(h) F_c(m) rint(Re X(m) / N^3)
-    SPEC_MASK_ADD = 4      // out += weight * F(m) X(m) where F selects (adjoint)
+    SPEC_MASK_ADD = 4,     // out += weight * F(m) X(m) where F selects (adjoint)
+    SPEC_DOT_ABS = 5       // as SPEC_DOT with |term| (condition numbers)
 };
 
 template <typename T, int N>
@@ -497,7 +505,8 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     const bool col_ok = h < hvalid && h <= N / 2;
     const int my = lattice_freq(j, N);
     const int mz = h == N / 2 ? -(N / 2) : h;
-    const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT;
+    const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT || epi == SPEC_DOT_ABS;
+    const bool use_dk = epi == SPEC_DOT || epi == SPEC_DOT_ABS;
     V a[G::R];
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
@@ -523,7 +532,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
                 }
             }
             bits[e] = b;
-            dv[e] = (b && epi == SPEC_DOT) ? dk[((size_t)i * N + j) * dk_stride + h] : czero<V>();
+            dv[e] = (b && use_dk) ? dk[((size_t)i * N + j) * dk_stride + h] : czero<V>();
         }
     }
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
@@ -578,9 +587,9 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         if (bits[e]) {
-            const double val = epi == SPEC_DOT
-                                   ? wgt * ((double)dv[e].x * (double)a[e].x + (double)dv[e].y * (double)a[e].y)
-                                   : wgt * rint((double)a[e].x * inv_n3);
+            double val = use_dk ? wgt * ((double)dv[e].x * (double)a[e].x + (double)dv[e].y * (double)a[e].y)
+                                : wgt * rint((double)a[e].x * inv_n3);
+            if (epi == SPEC_DOT_ABS) val = fabs(val);
 #pragma unroll
             for (int c = 0; c < MAX_DOT_SHELLS; c++)
                 if ((bits[e] >> c) & 1u) acc[c] += val;
@@ -647,6 +656,88 @@ __global__ void k_scale_out(const T* __restrict__ in, O* __restrict__ out, size_
 {
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < count; q += (size_t)gridDim.x * blockDim.x)
         out[q] = (O)(scale * (double)in[q]);
+}
+
+// ------------------------------------------------------------------ n = 2 (Parseval)
+// Per configuration c (legs a, b): S_D = N^3 sum_half w(h) F_a F_b |dk|^2 and
+// the count sum_half w(h) F_a F_b (exact), over the band cube |m| <= band.
+// The per-mode configuration bitmask comes from lut[r2] (interval shells) or
+// from the shell pairs legs[2c], legs[2c+1].  Per-thread FP64 sums, one
+// fixed-order reduction: partials[c] (sums) and partials[MAX + c] (counts).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_pair2_sums(int n, const V2<T>* __restrict__ dk, int dks, const unsigned short* __restrict__ lut, int lut_size,
+                 const Shell* __restrict__ legs, int ncfg, int band, double* __restrict__ partials)
+{
+    double acc[MAX_DOT_SHELLS], cnt[MAX_DOT_SHELLS];
+#pragma unroll
+    for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = cnt[c] = 0.0;
+    const int b = min(band, n / 2);
+    const int side = 2 * b + 1;
+    const long long total = (long long)side * side * (b + 1);
+    const double n3 = (double)n * (double)n * (double)n;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int h = (int)(q % (b + 1));
+        const long long r = q / (b + 1);
+        const int mx = (int)(r / side) - b, my = (int)(r % side) - b;
+        if (mx >= n / 2 || my >= n / 2) continue;  // +N/2 is the index of -N/2, visited as such
+        const int mz = h == n / 2 ? -(n / 2) : h;
+        unsigned bits = 0u;
+        if (lut) {
+            const int r2 = mx * mx + my * my + mz * mz;
+            bits = r2 < lut_size ? (unsigned)__ldg(lut + r2) : 0u;
+        } else {
+            for (int c = 0; c < ncfg; c++) {
+                const Shell& sa = legs[2 * c];
+                const Shell& sb = legs[2 * c + 1];
+                if (in_band(sa, mx, my, mz) && shell_bit(sa, mx, my, mz) && in_band(sb, mx, my, mz) &&
+                    shell_bit(sb, mx, my, mz))
+                    bits |= 1u << c;
+            }
+        }
+        if (!bits) continue;
+        const int i = mx < 0 ? mx + n : mx, j = my < 0 ? my + n : my;
+        const V2<T> d = dk[((size_t)i * n + j) * dks + h];
+        const double wgt = (double)herm_weight(h, n);
+        const double val = wgt * n3 * ((double)d.x * (double)d.x + (double)d.y * (double)d.y);
+#pragma unroll
+        for (int c = 0; c < MAX_DOT_SHELLS; c++)
+            if ((bits >> c) & 1u) {
+                acc[c] += val;
+                cnt[c] += wgt;
+            }
+    }
+    __shared__ double wsum[8][2 * MAX_DOT_SHELLS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < MAX_DOT_SHELLS; c++) {
+        double v = acc[c], u = cnt[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+            u += __shfl_xor_sync(0xffffffffu, u, o);
+        }
+        if (lane == c) {
+            wsum[wid][c] = v;
+            wsum[wid][MAX_DOT_SHELLS + c] = u;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * MAX_DOT_SHELLS) {
+        double sum = 0.0;
+#pragma unroll 1
+        for (int q = 0; q < 8; q++) sum += wsum[q][threadIdx.x];
+        partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = sum;
+    }
+}
+
+// dst[idx[q]] = src[q]
+static __global__ void k_scatter(const double* __restrict__ src, const int* __restrict__ idx, int count,
+                                 double* __restrict__ dst)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < count) dst[idx[q]] = src[q];
 }
 
 // ------------------------------------------------------------------ final sums

@@ -145,3 +145,36 @@ def test_device_resident_field(gpu_lib, ora):
             outs.append(ctx.batch(cfgs, ps.PS_FP32_BATCHED)[:2])
     np.testing.assert_array_equal(outs[0][0], outs[1][0])
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.parametrize("method", [1, 2], ids=["plain64", "batched32"])
+def test_condition_numbers(gpu_lib, method):
+    """kappa = sum|terms| / |sum terms| of the final sum: >= 1, finite, and 1 for
+    power spectra (all terms |dk|^2) in the batched method."""
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    dens, xhii = fields(n_grid, box)
+    cfgs, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=0.1, k2=0.14, num_values=5, kbinningCase=1)
+    with ps.Context(n_grid, box) as ctx:
+        ctx.get_FT_field(0, dens)
+        B, Np, kap, _ = ctx.batch(cfgs, method)
+        assert np.all(np.isfinite(kap)) and np.all(kap >= 1.0 - 1e-12), kap
+        p2, _, _ = ps.read_params_to_kvectors(n_grid, box, 2, num_values=2)
+        _, _, kap2, _ = ctx.batch(p2, method)
+        if method == 2:
+            assert np.all(kap2 == 1.0)
+        else:
+            assert np.all(kap2 >= 1.0 - 1e-12)
+
+
+def test_power_spectrum_sweep_many_shells(gpu_lib, ora):
+    """n = 2 over all N/2 shells (several Parseval passes of 16) at 64^3."""
+    ps = gpu_lib
+    n_grid, box = 64, 300.0
+    dens, _ = fields(n_grid, box)
+    case = dict(n=2, equilateral=0, k1=0.0, k2=0.0, num_values=2, theta=0.0, kbinwidth=1.0,
+                kbinning=0, dcos_theta=0.2, use_only_phase=0, which_field=0)
+    for method in (1, 2):
+        ref, got = run_both(ps, ora, n_grid, box, case, method)
+        assert len(got.k) == n_grid // 2
+        check(ref, got, method, f"pk m={method}")
