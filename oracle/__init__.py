@@ -11,10 +11,12 @@ bench.py import this package, and only as the checker.  Two libraries:
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import math
 import os
 import subprocess
+import sys
 import tempfile
 from dataclasses import dataclass, field
 
@@ -101,6 +103,24 @@ class RunResult:
     t_forward: float = math.nan
     t_configs: float = math.nan
     extra: dict = field(default_factory=dict)
+
+
+@contextlib.contextmanager
+def c_stdout_to_stderr():
+    """Send what C code prints on stdout (the reference's progress printf's,
+    e.g. polyspectrum.c:142, input_field.c:46) to stderr while the block runs,
+    so a caller's stdout carries only its own output."""
+    libc = C.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved = os.dup(1)
+    try:
+        os.dup2(2, 1)
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
 
 
 def _load(path: str) -> C.CDLL:
@@ -302,12 +322,14 @@ def ref_run(p: RunParams, dens, xhii=None, first: int = 0, count: int = -1) -> R
         np.ascontiguousarray(xhii if xhii is not None else zeros, dtype=dt).tofile(ipath)
         ini = os.path.join(td, "iniFile.ini")
         write_ini(ini, p, dpath, ipath, is_double, td)
-        total = lib.ref_num_configs_ini(ini.encode())
+        with c_stdout_to_stderr():
+            total = lib.ref_num_configs_ini(ini.encode())
         ncfg = total - first if count < 0 else min(count, total - first)
         out = [np.zeros(max(ncfg, 1)) for _ in range(4)] + \
               [np.zeros(max(ncfg, 1) * p.n) for _ in range(3)]
         tf, tc = C.c_double(), C.c_double()
-        got = lib.ref_run_ini(ini.encode(), first, ncfg, *out, C.byref(tf), C.byref(tc))
+        with c_stdout_to_stderr():
+            got = lib.ref_run_ini(ini.encode(), first, ncfg, *out, C.byref(tf), C.byref(tc))
     k, th, b, npol, kp, kl, kh = [o[: got * (p.n if i >= 4 else 1)] for i, o in enumerate(out)]
     return RunResult(k, th, b, npol, kp.reshape(got, p.n), kl.reshape(got, p.n),
                      kh.reshape(got, p.n), tf.value, tc.value)

@@ -206,8 +206,10 @@ class Context:
                                          kbinningCase, C.byref(B), C.byref(Np)))
         return B.value, Np.value, lo, hi
 
-    def batch(self, cfgs, method: int = PS_FP32_BATCHED):
-        """Evaluate a list of ps_cfg.  Returns (B, Npoly, kappa, cfgs-after)."""
+    def batch(self, cfgs, method: int = PS_FP32_BATCHED, kappa: bool = False):
+        """Evaluate a list of ps_cfg.  Returns (B, Npoly, kappa, cfgs-after);
+        kappa (condition numbers, one extra pass per sum) only when asked,
+        else NaN."""
         if not isinstance(cfgs, C.Array):
             arr = (ps_cfg * len(cfgs))(*cfgs)
         else:
@@ -215,9 +217,9 @@ class Context:
         m = len(arr)
         B = np.zeros(m)
         Np = np.zeros(m)
-        kap = np.zeros(m)
+        kap = np.full(m, np.nan)
         _check(lib().ps_gpu_polyspectrum_batch(self._h, method, m, arr, _dptr(B), _dptr(Np),
-                                               _dptr(kap)))
+                                               _dptr(kap) if kappa else None))
         return B, Np, kap, arr
 
     def grad(self, n, k, kmin, kmax, kbinwidth, kbinningCase, method=PS_FP64_PLAIN,

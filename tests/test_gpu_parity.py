@@ -157,10 +157,10 @@ def test_condition_numbers(gpu_lib, method):
     cfgs, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=0.1, k2=0.14, num_values=5, kbinningCase=1)
     with ps.Context(n_grid, box) as ctx:
         ctx.get_FT_field(0, dens)
-        B, Np, kap, _ = ctx.batch(cfgs, method)
+        B, Np, kap, _ = ctx.batch(cfgs, method, kappa=True)
         assert np.all(np.isfinite(kap)) and np.all(kap >= 1.0 - 1e-12), kap
         p2, _, _ = ps.read_params_to_kvectors(n_grid, box, 2, num_values=2)
-        _, _, kap2, _ = ctx.batch(p2, method)
+        _, _, kap2, _ = ctx.batch(p2, method, kappa=True)
         if method == 2:
             assert np.all(kap2 == 1.0)
         else:
