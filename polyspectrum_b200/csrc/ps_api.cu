@@ -359,7 +359,8 @@ int sum_partials(ps_gpu_ctx* c, int nblocks, int ncols, double* out, int out_str
 // the shell: h < hb = min(band, N/2) + 1 columns, row stride *S_out.
 // mode: LOAD_MASKED (F * field spectrum) or LOAD_UNIT (F).
 template <typename T>
-int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, int* S_out, int* hb_out)
+int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, int* S_out, int* hb_out,
+           int quad = 0)
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
@@ -368,13 +369,16 @@ int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, i
     const double V = sizeof(V2<T>), NN2 = (double)N * N;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, dst, S, mode, dshell, N / 2 + 1, B.tables()))));
-        pf.end(KF_INV_X, NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, dst, S, mode, dshell, N / 2 + 1, B.tables(),
+                                                quad))));
+        const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
+        pf.end(KF_INV_X, q * NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, B.tables()))));
-        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, B.tables(), quad))));
+        const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
+        pf.end(KF_PASS_Y, 2.0 * q * NN2 * S * V);
     }
     *S_out = S;
     *hb_out = hb;
@@ -412,21 +416,23 @@ int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, co
 // NULL: square of A), rows kept to h < hout, forward Y pass done; into B.work3.
 template <typename T>
 int pair_spectrum(ps_gpu_ctx* c, const V2<T>* A, int Sa, int hba, const V2<T>* Bq, int Sb, int hbb, int hout,
-                  int* S_out)
+                  int* S_out, int quad = 0)
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
     const int S = round_up(hout, pw<T>(N));
     const double V = sizeof(V2<T>), NN2 = (double)N * N;
+    const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, B.tables()))));
-        pf.end(KF_PAIR_Z, NN2 * (hba + (Bq ? hbb : 0) + hout) * V);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, B.tables(),
+                                                 quad))));
+        pf.end(KF_PAIR_Z, q * NN2 * (hba + (Bq ? hbb : 0) + hout) * V);
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, B.tables()))));
-        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, B.tables(), quad))));
+        pf.end(KF_PASS_Y, 2.0 * q * NN2 * S * V);
     }
     *S_out = S;
     return PS_OK;
@@ -490,7 +496,7 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
 // hsh: host copies of the shells (decide whether an r2 bitmask table applies).
 template <typename T>
 int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell* dshells,
-             const Shell* hsh, int ns, double* dout)
+             const Shell* hsh, int ns, double* dout, int quad = 0)
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
@@ -517,8 +523,10 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
         {
             Prof pf(c);
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, data, S, hvalid, epi, nullptr, 0, B.spec, B.S,
-                                                    dshells + s0, cnt, lut, lut_size, c->partials, B.tables(), &nb))));
-            pf.end(KF_FWD_X_DOT, (double)N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
+                                                    dshells + s0, cnt, lut, lut_size, c->partials, B.tables(), &nb,
+                                                    1.0, quad))));
+            const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / ((double)N * N) : 1.0;
+            pf.end(KF_FWD_X_DOT, q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
         }
         PS_TRY(sum_partials(c, nb, cnt, dout + s0, 1));
     }
@@ -973,10 +981,12 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, doubl
             PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, c->dshells + gofs[g], table.data() + gofs[g],
                                    ng, gA));
         // I part (FP64): the same on unit shells, counts rounded per mode
-        PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.work, &Sa, &ha));
-        if (G.a != G.b) PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.b, sb.band, c->d.work2, &Sb, &hbb));
-        PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S));
-        PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gI));
+        // (unit filters are even in every axis: the xy-quadrant carries everything)
+        PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.work, &Sa, &ha, 1));
+        if (G.a != G.b) PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.b, sb.band, c->d.work2, &Sb, &hbb, 1));
+        PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S, 1));
+        PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gI,
+                                1));
         PS_TRY(scatter(c, gD, G.cfg, sumD));
         PS_TRY(scatter(c, gI, G.cfg, sumI));
         if (kappa) PS_TRY(scatter(c, gA, G.cfg, sumA));

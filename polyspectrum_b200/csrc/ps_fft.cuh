@@ -118,10 +118,11 @@ struct BlockSync {
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
 template <int TPF> struct RowSync {
-    int bar;
+    int bar;         // named barrier id (TPF > 32)
+    unsigned mask;   // this row's lanes (TPF <= 32)
     __device__ __forceinline__ void operator()() const
     {
-        if constexpr (TPF <= 32) __syncwarp();
+        if constexpr (TPF <= 32) __syncwarp(mask);
         else asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(TPF) : "memory");
     }
 };

@@ -102,13 +102,14 @@ __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wa
 // 16-byte multiple, which stays inside the row stride ss) into `stage`
 // (pitch P) with the whole CTA.
 template <typename V, int WZ, int THREADS>
-__device__ __forceinline__ void stage_rows(V* stage, int P, const V* __restrict__ src, size_t row0, int ss, int hv)
+__device__ __forceinline__ void stage_rows(V* stage, int P, const V* __restrict__ src, size_t row0, int ss, int hv,
+                                           int nrows = 0x7fffffff)
 {
     constexpr int EPC = 16 / (int)sizeof(V);
     const int chunks = (hv + EPC - 1) / EPC;
     for (int c = threadIdx.x; c < WZ * chunks; c += THREADS) {
         const int w = c / chunks, q = c - w * chunks;
-        cp_async16(stage + w * P + q * EPC, src + (row0 + w) * ss + q * EPC);
+        if (row0 + w < (size_t)nrows) cp_async16(stage + w * P + q * EPC, src + (row0 + w) * ss + q * EPC);
     }
 }
 
@@ -137,7 +138,7 @@ enum InvLoad : int { LOAD_PLAIN = 0, LOAD_MASKED = 1, LOAD_UNIT = 2 };
 template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     k_inv_x(const V2<T>* __restrict__ src, int src_stride, V2<T>* __restrict__ dst, int dst_stride,
-            int mode, const Shell* __restrict__ shell_p, int hvalid, const V2<T>* __restrict__ tw_g)
+            int mode, const Shell* __restrict__ shell_p, int hvalid, int quad, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
@@ -147,6 +148,9 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), (int)(threadIdx.x % G::W)};
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
     const int tiles_per_row = dst_stride / G::W;
+    // quad: pencils j <= N/2 only, outputs i <= N/2 only, stored [i][j][h] with
+    // N/2+1 rows per plane (the unit filter is even in every axis)
+    const int nj = quad ? N / 2 + 1 : N;
     const int j = blockIdx.x / tiles_per_row;
     const int h = (blockIdx.x % tiles_per_row) * G::W + w;
     const int my = lattice_freq(j, N);
@@ -184,32 +188,41 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int i = t + G::TPF * e;
-        dst[((size_t)i * N + j) * dst_stride + h] = a[e];
+        if (!quad || i <= N / 2) dst[((size_t)i * nj + j) * dst_stride + h] = a[e];
     }
 }
 
 // ------------------------------------------------------------------ Y pass
 template <typename T, int N, bool INV>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
-    k_pass_y(V2<T>* __restrict__ data, int stride, const V2<T>* __restrict__ tw_g)
+    k_pass_y(V2<T>* __restrict__ data, int stride, int quad, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
     const int tiles_per_plane = stride / G::W;
+    // quad: planes i <= N/2, rows j <= N/2 stored, row N-j read as row j
+    // (data even in y)
+    const int nj = quad ? N / 2 + 1 : N;
     const int i = blockIdx.x / tiles_per_plane;
     const int h = (blockIdx.x % tiles_per_plane) * G::W + w;
-    V* base = data + (size_t)i * N * stride + h;
+    V* base = data + (size_t)i * nj * stride + h;
     V a[G::R];
 #pragma unroll
-    for (int e = 0; e < G::R; e++) a[e] = base[(size_t)(t + G::TPF * e) * stride];
+    for (int e = 0; e < G::R; e++) {
+        const int j = t + G::TPF * e;
+        a[e] = base[(size_t)(quad && j > N / 2 ? N - j : j) * stride];
+    }
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
     __syncthreads();
     SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), w};
     fft_passes<V, N, G::R, INV>(a, t, sm, tw, BlockSync{});
 #pragma unroll
-    for (int e = 0; e < G::R; e++) base[(size_t)(t + G::TPF * e) * stride] = a[e];
+    for (int e = 0; e < G::R; e++) {
+        const int j = t + G::TPF * e;
+        if (!quad || j <= N / 2) base[(size_t)j * stride] = a[e];
+    }
 }
 
 // ------------------------------------------------------------------ row helpers
@@ -233,6 +246,12 @@ template <typename T, int N> struct RowCtx {
         t = threadIdx.x % G::TPF;
         rowbuf = reinterpret_cast<V*>(smem + G::ROWBUF_OFF) + w * G::NH;
         sync.bar = 1 + w;
+        if constexpr (G::TPF >= 32) {
+            sync.mask = 0xffffffffu;
+        } else {
+            const int base = (threadIdx.x & 31) / G::TPF * G::TPF;
+            sync.mask = ((1u << G::TPF) - 1u) << base;
+        }
     }
 };
 
@@ -431,7 +450,7 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
 template <typename T, int N>
 __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
     k_pair_z(const V2<T>* __restrict__ srcA, int sa, int hva, const V2<T>* __restrict__ srcB, int sb,
-             int hvb, V2<T>* __restrict__ dst, int ds, int hout, const V2<T>* __restrict__ twr_g,
+             int hvb, V2<T>* __restrict__ dst, int ds, int hout, int nrows, const V2<T>* __restrict__ twr_g,
              const V2<T>* __restrict__ twpp_g)
 {
     using G = RowGeom<T, N>;
@@ -442,25 +461,30 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
     const int PA = G::pitch(hva), PB = two ? G::pitch(hvb) : 0;
     V* stA = reinterpret_cast<V*>(smem_raw + G::STAGE_OFF);
     V* stB = stA + 2 * G::WZ * PA;
-    const int ntiles = N * N / G::WZ;
+    const int ntiles = (nrows + G::WZ - 1) / G::WZ;
     int tile = blockIdx.x;
     if (tile < ntiles) {
-        stage_rows<V, G::WZ, G::THREADS>(stA, PA, srcA, (size_t)tile * G::WZ, sa, hva);
-        if (two) stage_rows<V, G::WZ, G::THREADS>(stB, PB, srcB, (size_t)tile * G::WZ, sb, hvb);
+        stage_rows<V, G::WZ, G::THREADS>(stA, PA, srcA, (size_t)tile * G::WZ, sa, hva, nrows);
+        if (two) stage_rows<V, G::WZ, G::THREADS>(stB, PB, srcB, (size_t)tile * G::WZ, sb, hvb, nrows);
     }
     cp_async_commit();
     for (int st = 0; tile < ntiles; tile += gridDim.x, st ^= 1) {
         const int next = tile + gridDim.x;
         if (next < ntiles) {
-            stage_rows<V, G::WZ, G::THREADS>(stA + (st ^ 1) * G::WZ * PA, PA, srcA, (size_t)next * G::WZ, sa, hva);
+            stage_rows<V, G::WZ, G::THREADS>(stA + (st ^ 1) * G::WZ * PA, PA, srcA, (size_t)next * G::WZ, sa, hva,
+                                             nrows);
             if (two)
                 stage_rows<V, G::WZ, G::THREADS>(stB + (st ^ 1) * G::WZ * PB, PB, srcB, (size_t)next * G::WZ, sb,
-                                                 hvb);
+                                                 hvb, nrows);
         }
         cp_async_commit();
         cp_async_wait_prev();
         __syncthreads();
         const size_t row = (size_t)tile * G::WZ + rc.w;
+        if (row >= (size_t)nrows) {  // whole row group idle in the last tile
+            __syncthreads();
+            continue;
+        }
         V a[G::R];
         c2r_row<T, N>(stA + st * G::WZ * PA + rc.w * PA, hva, rc, a);
         if (two) {
@@ -492,7 +516,7 @@ template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, const Shell* __restrict__ shells,
-            int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight,
+            int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight, int quad,
             double* __restrict__ partials, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
@@ -500,6 +524,9 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
     const int tiles_per_row = stride / G::W;
+    // quad (counts only): pencils j <= N/2 of data even in x and y stored
+    // [i <= N/2][j <= N/2][h]; plane N-i read as plane i; interior j weigh 2
+    const int nj = quad ? N / 2 + 1 : N;
     const int j = blockIdx.x / tiles_per_row;
     const int h = (blockIdx.x % tiles_per_row) * G::W + w;
     const bool col_ok = h < hvalid && h <= N / 2;
@@ -511,7 +538,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int i = t + G::TPF * e;
-        a[e] = data[((size_t)i * N + j) * stride + h];
+        a[e] = data[((size_t)(quad && i > N / 2 ? N - i : i) * nj + j) * stride + h];
     }
     // dot / count: the shell bits depend on indices only, so they and the
     // field values they need are fetched before the transform
@@ -582,7 +609,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     double acc[MAX_DOT_SHELLS];
 #pragma unroll
     for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = 0.0;
-    const double wgt = (double)herm_weight(h, N);
+    const double wgt = (double)(herm_weight(h, N) * (quad && j != 0 && j != N / 2 ? 2 : 1));
     const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
 #pragma unroll
     for (int e = 0; e < G::R; e++) {

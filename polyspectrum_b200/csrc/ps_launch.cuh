@@ -70,23 +70,26 @@ template <typename T, int N> struct L3 {
         stockham_table<V, N, PG::R>(twp);
         stockham_table<V, N / 2, RG::R>(twr);
     }
+    // quad: the xy-quadrant layout of data even in x and y ([i <= N/2][j <= N/2][h])
     static int inv_x(cudaStream_t st, const V* src, int ss, V* dst, int ds, int mode, const Shell* sh,
-                     int hvalid, const Tables<T>& tb)
+                     int hvalid, const Tables<T>& tb, int quad = 0)
     {
         PS_LTRY(set_smem(k_inv_x<T, N>, PG::SMEM));
-        k_inv_x<T, N><<<(unsigned)(N * (ds / PG::W)), PG::THREADS, PG::SMEM, st>>>(
-            src, ss, dst, ds, mode, sh, hvalid, tb.twp);
+        const int nj = quad ? N / 2 + 1 : N;
+        k_inv_x<T, N><<<(unsigned)(nj * (ds / PG::W)), PG::THREADS, PG::SMEM, st>>>(
+            src, ss, dst, ds, mode, sh, hvalid, quad, tb.twp);
         return PS_OK;
     }
-    static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb)
+    static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb, int quad = 0)
     {
-        const unsigned blocks = (unsigned)(N * (stride / PG::W));
+        const int ni = quad ? N / 2 + 1 : N;
+        const unsigned blocks = (unsigned)(ni * (stride / PG::W));
         if (inv) {
             PS_LTRY(set_smem(k_pass_y<T, N, true>, PG::SMEM));
-            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, tb.twp);
+            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, tb.twp);
         } else {
             PS_LTRY(set_smem(k_pass_y<T, N, false>, PG::SMEM));
-            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, tb.twp);
+            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, tb.twp);
         }
         return PS_OK;
     }
@@ -112,23 +115,27 @@ template <typename T, int N> struct L3 {
         return PS_OK;
     }
     static int pair_z(cudaStream_t st, const V* a, int sa, int hva, const V* b, int sb, int hvb, V* dst,
-                      int ds, int hout, const Tables<T>& tb)
+                      int ds, int hout, const Tables<T>& tb, int quad = 0)
     {
         const size_t smem = RG::smem(b ? 2 : 1, hva, hvb);
         PS_LTRY(set_smem(k_pair_z<T, N>, RG::smem(2, N / 2 + 1, N / 2 + 1)));
+        const int nrows = quad ? (N / 2 + 1) * (N / 2 + 1) : N * N;
         int grid = 0;
-        PS_LTRY(persistent_grid(k_pair_z<T, N>, RG::THREADS, smem, N * N / RG::WZ, &grid));
-        k_pair_z<T, N><<<grid, RG::THREADS, smem, st>>>(a, sa, hva, b, sb, hvb, dst, ds, hout, tb.twr, tb.twpp);
+        PS_LTRY(persistent_grid(k_pair_z<T, N>, RG::THREADS, smem, (nrows + RG::WZ - 1) / RG::WZ, &grid));
+        k_pair_z<T, N><<<grid, RG::THREADS, smem, st>>>(a, sa, hva, b, sb, hvb, dst, ds, hout, nrows, tb.twr,
+                                                        tb.twpp);
         return PS_OK;
     }
     static int fwd_x(cudaStream_t st, V* data, int stride, int hvalid, int epi, V* out, int ostride,
                      const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
-                     int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0)
+                     int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0,
+                     int quad = 0)
     {
         PS_LTRY(set_smem(k_fwd_x<T, N>, PG::SMEM));
-        const unsigned blocks = (unsigned)(N * (stride / PG::W));
+        const int nj = quad ? N / 2 + 1 : N;
+        const unsigned blocks = (unsigned)(nj * (stride / PG::W));
         k_fwd_x<T, N><<<blocks, PG::THREADS, PG::SMEM, st>>>(
-            data, stride, hvalid, epi, out, ostride, dk, dks, shells, nshell, lut, lut_size, weight, partials,
+            data, stride, hvalid, epi, out, ostride, dk, dks, shells, nshell, lut, lut_size, weight, quad, partials,
             tb.twp);
         if (nblocks) *nblocks = (int)blocks;
         return PS_OK;
