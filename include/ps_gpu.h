@@ -130,6 +130,53 @@ int ps_gpu_polyspectrum(ps_gpu_ctx *ctx, int n, const double *k, double *kmin, d
 int ps_gpu_polyspectrum_batch(ps_gpu_ctx *ctx, int method, int nconf, ps_cfg *cfgs, double *B,
                               double *Npoly, double *kappa_or_NULL);
 
+/* A batch prepared once and executed many times (for example once per field
+ * of a simulation series).  Planning does all host work: legs are resolved to
+ * shells and deduplicated, configurations are grouped, tables are uploaded and
+ * scratch is sized; DERIVED k ranges and closing-leg shells are finished on the
+ * device during execution.  Execution is stream work only, so with
+ * PS_PLAN_GRAPH the first execution captures it into a CUDA graph that later
+ * executions replay.  A plan belongs to the context it was created on and
+ * uses the field most recently loaded into it.  PS_PLAN_KAPPA adds the
+ * condition-number passes.  PS_FP64_PLAIN plans evaluate their configurations
+ * one by one (no graph). */
+#define PS_PLAN_GRAPH 1
+#define PS_PLAN_KAPPA 2
+typedef struct ps_gpu_plan ps_gpu_plan;
+int ps_gpu_plan_create(ps_gpu_ctx *ctx, int method, int nconf, const ps_cfg *cfgs, int flags,
+                       ps_gpu_plan **plan);
+/* B, Npoly (and kappa when the plan has PS_PLAN_KAPPA) per configuration;
+ * cfgs_out_or_NULL receives the configurations with DERIVED ranges written
+ * back, as ps_gpu_polyspectrum_batch writes them. */
+int ps_gpu_plan_execute(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
+                        double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
+/* Frees the plan (waits for its submissions).  Destroy plans before their
+ * context; a plan that outlives its context holds no device memory and can
+ * only be destroyed. */
+void ps_gpu_plan_destroy(ps_gpu_plan *plan);
+
+/* Asynchronous pipeline over a series of fields (no reference counterpart:
+ * the reference runs one process per field).  ps_gpu_set_field_async is
+ * ps_gpu_set_field without waiting: host arrays are copied on the context's
+ * copy stream into one of two device staging slots, and the forward transform
+ * is queued on the compute stream behind that copy.  ps_gpu_plan_submit queues
+ * a PS_FP32_BATCHED plan execution behind it; its results reach B, Npoly (and
+ * kappa, cfgs_out) in stream order, by a host callback.  So the upload of
+ * field k+1 overlaps the configurations of field k.  Every pointer passed to
+ * these two calls (inputs and outputs) must stay valid and the inputs
+ * unchanged until ps_gpu_synchronize returns; host inputs overlap only when
+ * they are page-locked (cudaHostAlloc / cudaHostRegister).  Errors detected on
+ * the device during a submission are returned by ps_gpu_synchronize. */
+int ps_gpu_set_field_async(ps_gpu_ctx *ctx, int which, const void *dens, const void *xhii,
+                           int is_double, int mem, int use_only_phase);
+int ps_gpu_plan_submit(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
+                       double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
+int ps_gpu_synchronize(ps_gpu_ctx *ctx);
+
+/* Kernels the context has executed since its creation (a graph replay counts
+ * the kernels in the graph); -1 for a NULL context. */
+long long ps_gpu_launch_count(ps_gpu_ctx *ctx);
+
 /* Gradient dB/d(delta) of one configuration with respect to the real input
  * field (the array the forward transform read), written to out as N^3 float
  * (out_is_double = 0) or double (1) in host or device memory (out_mem).  No

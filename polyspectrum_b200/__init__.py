@@ -79,6 +79,15 @@ def lib() -> C.CDLL:
     L.ps_make_configs.argtypes = [C.POINTER(ps_run_params), C.POINTER(ps_cfg), ip, dp, dp]
     L.ps_gpu_set_stream.argtypes = [vp, vp]
     L.ps_gpu_last_timing.argtypes = [vp, dp, C.POINTER(C.c_longlong)]
+    L.ps_gpu_plan_create.argtypes = [vp, ip, ip, C.POINTER(ps_cfg), ip, C.POINTER(vp)]
+    L.ps_gpu_plan_execute.argtypes = [vp, vp, dp, dp, dp, C.POINTER(ps_cfg)]
+    L.ps_gpu_plan_destroy.argtypes = [vp]
+    L.ps_gpu_plan_destroy.restype = None
+    L.ps_gpu_set_field_async.argtypes = [vp, ip, vp, vp, ip, ip, ip]
+    L.ps_gpu_plan_submit.argtypes = [vp, vp, dp, dp, dp, C.POINTER(ps_cfg)]
+    L.ps_gpu_synchronize.argtypes = [vp]
+    L.ps_gpu_launch_count.argtypes = [vp]
+    L.ps_gpu_launch_count.restype = C.c_longlong
     L.ps_gpu_set_profiling.argtypes = [vp, ip]
     L.ps_gpu_kernel_stats.argtypes = [vp, C.POINTER(ps_kernel_stat), ip]
     L.ps_gpu_finalize.argtypes = [vp]
@@ -90,7 +99,8 @@ def lib() -> C.CDLL:
     for name in ("ps_gpu_create", "ps_gpu_set_field", "ps_gpu_init", "ps_gpu_polyspectrum",
                  "ps_gpu_polyspectrum_batch", "ps_gpu_grad", "ps_make_configs",
                  "ps_gpu_set_stream", "ps_gpu_last_timing", "ps_gpu_set_profiling",
-                 "ps_gpu_kernel_stats"):
+                 "ps_gpu_kernel_stats", "ps_gpu_plan_create", "ps_gpu_plan_execute",
+                 "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize"):
         getattr(L, name).restype = ip
     _lib = L
     return L
@@ -160,11 +170,13 @@ class Context:
         h = C.c_void_p()
         _check(lib().ps_gpu_create(C.byref(h), nbins, self.boxsize, methods, device))
         self._h = h
+        self._inflight = []  # arrays an asynchronous call may still read or write
 
     def close(self):
         if getattr(self, "_h", None):
             lib().ps_gpu_finalize(self._h)
             self._h = None
+            self._inflight = []
 
     def __del__(self):
         try:
@@ -194,6 +206,31 @@ class Context:
 
     set_field = get_FT_field
 
+    def set_field_async(self, which: int, dens=None, xhii=None, use_only_phase: int = 0):
+        """get_FT_field queued behind the work already on the context
+        (ps_gpu_set_field_async); the arrays are kept alive until synchronize().
+        Host arrays overlap with device work only when page-locked (torch
+        tensors from pin_memory())."""
+        pd, dd, md, kd = _field_ptr(dens)
+        px, dx, mx, kx = _field_ptr(xhii)
+        is_double = dd if dd is not None else dx
+        mem = md if md is not None else mx
+        if dd is not None and dx is not None and (dd != dx or md != mx):
+            raise ValueError("dens and xhii must share dtype and memory kind")
+        self._inflight.append((kd, kx))
+        _check(lib().ps_gpu_set_field_async(self._h, which, pd, px, is_double, mem, use_only_phase))
+
+    def synchronize(self):
+        """Wait for all queued work; raises for errors found during submissions."""
+        try:
+            _check(lib().ps_gpu_synchronize(self._h))
+        finally:
+            self._inflight = []
+
+    def launch_count(self) -> int:
+        """Kernels executed by this context since its creation."""
+        return int(lib().ps_gpu_launch_count(self._h))
+
     def polyspectrum(self, n, k, kmin, kmax, kbinwidth, kbinningCase):
         """polyspectrum() + num_polygons() of one configuration with the
         context's first method.  Returns (B, Npoly, kmin, kmax) (the k ranges
@@ -221,6 +258,10 @@ class Context:
         _check(lib().ps_gpu_polyspectrum_batch(self._h, method, m, arr, _dptr(B), _dptr(Np),
                                                _dptr(kap) if kappa else None))
         return B, Np, kap, arr
+
+    def plan(self, cfgs, method: int = PS_FP32_BATCHED, graph: bool = True, kappa: bool = False):
+        """A reusable plan of these configurations (ps_gpu_plan_create)."""
+        return Plan(self, cfgs, method, graph, kappa)
 
     def grad(self, n, k, kmin, kmax, kbinwidth, kbinningCase, method=PS_FP64_PLAIN,
              out=None, double=True):
@@ -252,6 +293,64 @@ class Context:
 
     def set_stream(self, stream_ptr: int | None):
         _check(lib().ps_gpu_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+
+PS_PLAN_GRAPH = 1
+PS_PLAN_KAPPA = 2
+
+
+class Plan:
+    """ps_gpu_plan: a batch planned once, executed per field (CUDA graph replay
+    with graph=True)."""
+
+    def __init__(self, ctx: Context, cfgs, method=PS_FP32_BATCHED, graph=True, kappa=False):
+        arr = cfgs if isinstance(cfgs, C.Array) else (ps_cfg * len(cfgs))(*cfgs)
+        self.ctx = ctx
+        self.n = len(arr)
+        self.kappa = kappa
+        h = C.c_void_p()
+        flags = (PS_PLAN_GRAPH if graph else 0) | (PS_PLAN_KAPPA if kappa else 0)
+        _check(lib().ps_gpu_plan_create(ctx.handle, method, self.n, arr, flags, C.byref(h)))
+        self._h = h
+
+    def execute(self):
+        B = np.zeros(self.n)
+        Np = np.zeros(self.n)
+        kap = np.full(self.n, np.nan)
+        out = (ps_cfg * max(self.n, 1))()
+        _check(lib().ps_gpu_plan_execute(self.ctx.handle, self._h, _dptr(B), _dptr(Np),
+                                         _dptr(kap) if self.kappa else None, out))
+        return B, Np, kap, out
+
+    def submit(self) -> "Submission":
+        """Queue one execution on the field most recently loaded (ps_gpu_plan_submit);
+        the returned arrays are filled once ctx.synchronize() returns."""
+        sub = Submission(self.n, self.kappa)
+        _check(lib().ps_gpu_plan_submit(self.ctx.handle, self._h, _dptr(sub.B), _dptr(sub.npoly),
+                                        _dptr(sub.kappa) if self.kappa else None, sub.cfgs))
+        self.ctx._inflight.append(sub)
+        return sub
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ps_gpu_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Submission:
+    """Output arrays of one asynchronous plan execution."""
+
+    def __init__(self, n: int, kappa: bool):
+        self.B = np.zeros(n)
+        self.npoly = np.zeros(n)
+        self.kappa = np.full(n, np.nan)
+        self.cfgs = (ps_cfg * max(n, 1))()
 
 
 @dataclass

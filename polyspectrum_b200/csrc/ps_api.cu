@@ -7,7 +7,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <functional>
 #include <map>
+#include <set>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -101,13 +104,23 @@ struct ps_gpu_ctx {
     size_t dminmax_cap = 0;
     unsigned short* dlut = nullptr;  // r2 -> shell bitmask
     size_t dlut_cap = 0;
-    int* didx = nullptr;  // scatter indices
-    size_t didx_cap = 0;
-    void* stage[2] = {nullptr, nullptr};
+    // scratch buffers replaced by larger ones stay allocated until finalize:
+    // a captured plan graph may still point at them
+    std::vector<void*> retired;
+    bool capturing = false;  // inside a plan graph capture: no profiling events
+    // host uploads: two staging slots of (dens, xhii), filled on copy_stream;
+    // ev_copied[s] = slot s filled, ev_free[s] = its forward transform is done
+    void* stage[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     size_t stage_bytes = 0;
+    int slot = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+    std::atomic<int> async_err{0};  // status of work whose results arrived in a host callback
+    std::set<ps_gpu_plan*> plans;   // live plans (finalize releases their device memory)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     long long launches = 0;
+    long long launches_total = 0;  // kernels executed since creation (graph replays included)
     int use_only_phase = 0;
     bool field_set = false;
     // per-kernel profiling (ps_gpu_set_profiling)
@@ -213,7 +226,7 @@ template <typename T> int ensure_pair_bufs(ps_gpu_ctx* c, PrecBufs<T>& b)
 int ensure_partials(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->partials_cap) return PS_OK;
-    cudaFree(c->partials);
+    if (c->partials) c->retired.push_back(c->partials);
     c->partials = nullptr;
     c->partials_cap = 0;
     PS_TRY(alloc_dev(&c->partials, n));
@@ -223,7 +236,7 @@ int ensure_partials(ps_gpu_ctx* c, size_t n)
 int ensure_sums(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->dsums_cap) return PS_OK;
-    cudaFree(c->dsums);
+    if (c->dsums) c->retired.push_back(c->dsums);
     c->dsums = nullptr;
     c->dsums_cap = 0;
     PS_TRY(alloc_dev(&c->dsums, n));
@@ -233,7 +246,7 @@ int ensure_sums(ps_gpu_ctx* c, size_t n)
 int ensure_shells(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->dshells_cap) return PS_OK;
-    cudaFree(c->dshells);
+    if (c->dshells) c->retired.push_back(c->dshells);
     c->dshells = nullptr;
     c->dshells_cap = 0;
     PS_TRY(alloc_dev(&c->dshells, n));
@@ -243,27 +256,17 @@ int ensure_shells(ps_gpu_ctx* c, size_t n)
 int ensure_lut(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->dlut_cap) return PS_OK;
-    cudaFree(c->dlut);
+    if (c->dlut) c->retired.push_back(c->dlut);
     c->dlut = nullptr;
     c->dlut_cap = 0;
     PS_TRY(alloc_dev(&c->dlut, n));
     c->dlut_cap = n;
     return PS_OK;
 }
-int ensure_idx(ps_gpu_ctx* c, size_t n)
-{
-    if (n <= c->didx_cap) return PS_OK;
-    cudaFree(c->didx);
-    c->didx = nullptr;
-    c->didx_cap = 0;
-    PS_TRY(alloc_dev(&c->didx, n));
-    c->didx_cap = n;
-    return PS_OK;
-}
 int ensure_minmax(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->dminmax_cap) return PS_OK;
-    cudaFree(c->dminmax);
+    if (c->dminmax) c->retired.push_back(c->dminmax);
     c->dminmax = nullptr;
     c->dminmax_cap = 0;
     PS_TRY(alloc_dev(&c->dminmax, n));
@@ -330,7 +333,7 @@ struct Prof {
     cudaEvent_t a = nullptr;
     explicit Prof(ps_gpu_ctx* cc) : c(cc)
     {
-        if (c->prof_on) {
+        if (c->prof_on && !c->capturing) {
             if (c->prof.size() >= 4096) prof_fold(c);
             a = prof_event(c);
             if (a) cudaEventRecord(a, c->stream);
@@ -339,6 +342,7 @@ struct Prof {
     void end(int kind, double bytes)
     {
         c->launches++;
+        if (!c->capturing) c->launches_total++;
         if (!a) return;
         cudaEvent_t b = prof_event(c);
         if (!b) return;
@@ -810,98 +814,264 @@ struct Group {  // n=3 configurations sharing the leg pair (a, b)
     std::vector<int> third;  // shell id of each configuration's remaining leg
 };
 
-// dst[idx[q]] = src[q], q < count (idx uploaded from the host).
-int scatter(ps_gpu_ctx* c, const double* src, const std::vector<int>& idx, double* dst)
+// The closing leg of a DERIVED configuration: its RANGE shell follows from the
+// device-derived ranges of legs 0 and 1 (calc_k3_min_and_max, filter.c:291-319).
+struct ClosingDesc {
+    int cfg;   // configuration (write-back row)
+    int d0;    // derived-range slots of legs 0 and 1
+    int d1;
+    int slot;  // shell-table slot to fill
+    int band;  // host upper bound of the shell's extent (launch geometry)
+    int pad;
+    double k0, k1, k2, half;
+};
+
+// kmin, kmax = sqrt(min / max corner^2) * 2 * PI / L (filter.c:112-113, same order)
+__global__ void k_derive_finish(int nd, const unsigned long long* __restrict__ mm, double pi, double L,
+                                double* __restrict__ kr)
 {
-    if (idx.empty()) return PS_OK;
-    PS_TRY(ensure_idx(c, idx.size()));
-    PS_CK(cudaMemcpyAsync(c->didx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, c->stream));
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nd) return;
+    const double rmin = __dsqrt_rn(__longlong_as_double((long long)mm[2 * s]));
+    const double rmax = __dsqrt_rn(__longlong_as_double((long long)mm[2 * s + 1]));
+    kr[2 * s] = __ddiv_rn(__dmul_rn(__dmul_rn(rmin, 2.0), pi), L);
+    kr[2 * s + 1] = __ddiv_rn(__dmul_rn(__dmul_rn(rmax, 2.0), pi), L);
+}
+
+__device__ __forceinline__ double k3_term(double a, double b, double c)  // a*a + b*b - 2.*a*b*c
+{
+    return __dsub_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(__dmul_rn(__dmul_rn(2.0, a), b), c));
+}
+
+// Closing-leg shells of DERIVED configurations (calc_k3_min_and_max, then
+// construct_kfilter_with_kbinwidth's mmin/mmax), written into the shell table,
+// and the derived k ranges of all three legs for the write-back.
+__global__ void k_closing(int ncl, const ClosingDesc* __restrict__ cd, const double* __restrict__ kr,
+                          Shell* __restrict__ table, double* __restrict__ wb, double pi, double L, int n,
+                          double min2_init, int* __restrict__ err)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ncl) return;
+    const ClosingDesc d = cd[q];
+    const double kmin0 = kr[2 * d.d0], kmax0 = kr[2 * d.d0 + 1];
+    const double kmin1 = kr[2 * d.d1], kmax1 = kr[2 * d.d1 + 1];
+    const double k0 = d.k0, k1 = d.k1, k2 = d.k2;
+    const double cth = __ddiv_rn(__dsub_rn(__dadd_rn(__dmul_rn(k0, k0), __dmul_rn(k1, k1)), __dmul_rn(k2, k2)),
+                                 __dmul_rn(__dmul_rn(2.0, k0), k1));
+    const double a[8] = {kmin0, kmin0, kmax0, kmax0, k0, kmax0, k0, kmin0};
+    const double b[8] = {kmin1, kmax1, kmin1, kmax1, kmax1, k1, kmin1, k1};
+    double lo = 1.e30, hi = 0.;
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+        const double v = k3_term(a[t], b[t], cth);
+        if (v < lo) lo = v;
+        if (v > hi) hi = v;
+    }
+    const double kmin2 = __dsqrt_rn(lo), kmax2 = __dsqrt_rn(hi);
+    Shell s;
+    s.kind = SHELL_RANGE;
+    s.band = d.band;
+    s.kk = 0.0;
+    s.half = d.half;
+    s.min2_init = min2_init;
+    const double twopi = __dmul_rn(2.0, pi);
+    s.mmin = __dmul_rn(__ddiv_rn(kmin2, twopi), L);  // filter.c:137-138
+    s.mmax = __dmul_rn(__ddiv_rn(kmax2, twopi), L);
+    shell_r2_interval(s, n);
+    // a band of N/2 holds every column; a narrower one must hold the whole shell
+    if (s.r2hi >= 0 && d.band < n / 2 && (long long)s.r2hi > (long long)d.band * d.band) atomicExch(err, 1);
+    table[d.slot] = s;
+    double* w = wb + 6 * (size_t)d.cfg;
+    w[0] = kmin0;
+    w[1] = kmax0;
+    w[2] = kmin1;
+    w[3] = kmax1;
+    w[4] = kmin2;
+    w[5] = kmax2;
+}
+
+__global__ void k_copy_shells(int n, const int* __restrict__ src, const int* __restrict__ dst, Shell* table)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) table[dst[q]] = table[src[q]];
+}
+
+// leg-by-leg configurations hold grid sums: count = rint(sum / N^3), exact
+// (the FP64 error is far below 1/2)
+__global__ void k_round_counts(int n, const int* __restrict__ idx, double* __restrict__ sumI, double n3)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) sumI[idx[q]] = rint(sumI[idx[q]] / n3);
+}
+
+}  // namespace
+
+// A batch prepared once: host planning, device tables and the launch sequence.
+struct ps_gpu_plan {
+    ps_gpu_ctx* ctx = nullptr;
+    int method = 0, nconf = 0, flags = 0;
+    std::vector<ps_cfg> cfgs;
+    std::vector<std::function<int()>> ops;  // the launch sequence (stream work only)
+    std::vector<void*> owned;               // device buffers of this plan
+    double* dres = nullptr;                 // B, Npoly per configuration
+    double* dsumA = nullptr;                // sum |terms| (condition numbers)
+    double* dsumD = nullptr;
+    double* dwb = nullptr;                  // derived k ranges, 6 per configuration
+    int* derr = nullptr;
+    double* hres = nullptr;  // pinned host copy of dres | dwb | dsumA | dsumD | err
+    std::vector<int> derived_cfgs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long graph_launches = 0;  // kernels in the captured graph
+};
+
+namespace {
+
+template <typename T> int plan_alloc(ps_gpu_plan* P, T** p, size_t count)
+{
+    *p = nullptr;
+    PS_TRY(alloc_dev(p, count));
+    P->owned.push_back(*p);
+    return PS_OK;
+}
+
+template <typename T> int plan_upload(ps_gpu_plan* P, T** p, const std::vector<T>& h)
+{
+    PS_TRY(plan_alloc(P, p, std::max<size_t>(h.size(), 1)));
+    if (!h.empty()) PS_CK(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    return PS_OK;
+}
+
+struct LegKey {
+    int tag;  // 0: exact host shell (bytes), 1: DERIVED closing leg
+    Shell sh;
+    double k0, k1, k2, half;
+    bool same(const LegKey& o) const
+    {
+        if (tag != o.tag) return false;
+        if (tag == 0) return memcmp(&sh, &o.sh, sizeof(Shell)) == 0;
+        return k0 == o.k0 && k1 == o.k1 && k2 == o.k2 && half == o.half;
+    }
+};
+
+int sum_partials_n(ps_gpu_ctx* c, int nblocks, int ncols, double* out)
+{
+    return sum_partials(c, nblocks, ncols, out, 1);
+}
+
+int scatter_dev(ps_gpu_ctx* c, const double* src, const int* didx, int count, double* dst)
+{
     Prof pf(c);
-    k_scatter<<<((int)idx.size() + 127) / 128, 128, 0, c->stream>>>(src, c->didx, (int)idx.size(), dst);
-    pf.end(KF_SUM, 16.0 * idx.size());
+    k_scatter<<<(count + 127) / 128, 128, 0, c->stream>>>(src, didx, count, dst);
+    pf.end(KF_SUM, 16.0 * count);
     return PS_OK;
 }
 
-// n = 2 configurations: sum_x D_a D_b = N^3 sum_m F_a F_b |dk|^2 and the exact
-// count of shared modes, one k-space pass per MAX_DOT_SHELLS configurations.
-int pair2_sums(ps_gpu_ctx* c, const std::vector<int>& qs, const std::vector<std::vector<int>>& lid,
-               const std::vector<Shell>& uniq, double* sumD, double* sumI, double* scratch)
+// Plan of the batched method: everything host-side happens here; the ops only
+// enqueue stream work (so a plan can be captured into a CUDA graph).
+int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
 {
+    if (!(c->methods & PS_FP32_BATCHED)) return fail(PS_ERR_ARG, "batched method not enabled for this context");
     const int N = c->N;
-    for (size_t q0 = 0; q0 < qs.size(); q0 += MAX_DOT_SHELLS) {
-        const int cnt = (int)std::min<size_t>(MAX_DOT_SHELLS, qs.size() - q0);
-        std::vector<Shell> pairs;  // legs of each configuration, then the interval pseudo-shells
-        bool lut_ok = true;
-        int band = 0, lut_size = 0;
-        for (int x = 0; x < cnt; x++) {
-            const Shell& sa = uniq[lid[qs[q0 + x]][0]];
-            const Shell& sb = uniq[lid[qs[q0 + x]][1]];
-            pairs.push_back(sa);
-            pairs.push_back(sb);
-            band = std::max(band, std::min(sa.band, sb.band));
-            if (sa.kind > SHELL_RANGE || sb.kind > SHELL_RANGE) lut_ok = false;
-        }
-        for (int x = 0; x < cnt && lut_ok; x++) {
-            Shell iv = pairs[2 * x];
-            iv.r2lo = std::max(pairs[2 * x].r2lo, pairs[2 * x + 1].r2lo);
-            iv.r2hi = std::min(pairs[2 * x].r2hi, pairs[2 * x + 1].r2hi);
-            lut_size = std::max(lut_size, iv.r2hi + 1);
-            pairs.push_back(iv);
-        }
-        PS_TRY(ensure_shells(c, pairs.size()));
-        PS_CK(cudaMemcpyAsync(c->dshells, pairs.data(), sizeof(Shell) * pairs.size(), cudaMemcpyHostToDevice,
-                              c->stream));
-        const unsigned short* lut = nullptr;
-        if (lut_ok) {
-            PS_TRY(ensure_lut(c, (size_t)std::max(lut_size, 1)));
-            Prof pf(c);
-            if (lut_size > 0)
-                k_shell_lut<<<(lut_size + 255) / 256, 256, 0, c->stream>>>(c->dshells + 2 * cnt, cnt, lut_size,
-                                                                           c->dlut);
-            pf.end(KF_LUT, 2.0 * lut_size);
-            lut = c->dlut;
-        }
-        const int b = std::min(band, N / 2);
-        const long long modes = (long long)(2 * b + 1) * (2 * b + 1) * (b + 1);
-        const int blocks = (int)std::max<long long>(1, std::min<long long>((modes + 255) / 256, 148 * 8));
-        PS_TRY(ensure_partials(c, (size_t)blocks * 2 * MAX_DOT_SHELLS));
-        {
-            Prof pf(c);
-            k_pair2_sums<float><<<blocks, 256, 0, c->stream>>>(N, c->f.spec, c->f.S, lut, lut_size, c->dshells, cnt,
-                                                               b, c->partials);
-            pf.end(KF_PAIR2, (double)modes * sizeof(V2<float>));
-        }
-        PS_TRY(sum_partials(c, blocks, 2 * MAX_DOT_SHELLS, scratch, 1));
-        std::vector<int> idx(qs.begin() + q0, qs.begin() + q0 + cnt);
-        PS_TRY(scatter(c, scratch, idx, sumD));
-        PS_TRY(scatter(c, scratch + MAX_DOT_SHELLS, idx, sumI));
-    }
-    PS_CK(cudaGetLastError());
-    return PS_OK;
-}
+    const double L = c->L;
+    const int nconf = P->nconf;
+    std::vector<ps_cfg>& cfgs = P->cfgs;
+    const bool kappa = (P->flags & PS_PLAN_KAPPA) != 0;
 
-int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, double* kappa)
-{
-    if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available (methods mask)");
-    const int N = c->N;
-    std::vector<std::vector<Shell>> legs;
-    PS_TRY(resolve_legs(c, nconf, cfgs, legs));
-    // unique shells
-    std::vector<Shell> uniq;
+    // ---- legs -> shells (DERIVED closing legs are completed on the device)
+    std::vector<LegKey> uniq;
     std::vector<std::vector<int>> lid(nconf);
+    std::vector<Shell> derived;  // DEFAULT shells whose DERIVED range is needed
+    std::vector<ClosingDesc> closing;
+    auto derived_slot = [&](const Shell& sh) {
+        for (size_t q = 0; q < derived.size(); q++)
+            if (memcmp(&derived[q], &sh, sizeof(Shell)) == 0) return (int)q;
+        derived.push_back(sh);
+        return (int)derived.size() - 1;
+    };
+    auto uniq_id = [&](const LegKey& k) {
+        for (size_t u = 0; u < uniq.size(); u++)
+            if (uniq[u].same(k)) return (int)u;
+        uniq.push_back(k);
+        return (int)uniq.size() - 1;
+    };
     for (int q = 0; q < nconf; q++) {
-        for (const Shell& s : legs[q]) {
-            int id = -1;
-            for (size_t u = 0; u < uniq.size(); u++)
-                if (same_shell(uniq[u], s)) { id = (int)u; break; }
-            if (id < 0) { id = (int)uniq.size(); uniq.push_back(s); }
-            lid[q].push_back(id);
+        const ps_cfg& g = cfgs[q];
+        if (g.n < 2 || g.n > PS_MAX_LEGS) return fail(PS_ERR_ARG, "config %d: n=%d out of range", q, g.n);
+        if (g.kbinningCase == PS_BIN_DERIVED && g.n != 3)
+            return fail(PS_ERR_UNDEFINED,
+                        "config %d: DERIVED binning with n=%d is undefined in the reference "
+                        "(calc_kn_min_and_max, filter.c:321-325)", q, g.n);
+        for (int l = 0; l < g.n; l++) {
+            const bool last = l == g.n - 1;
+            LegKey key;
+            memset(&key, 0, sizeof(key));
+            switch (g.kbinningCase) {
+            case PS_BIN_DERIVED:
+                if (!last) {
+                    key.sh = make_shell(SHELL_DEFAULT, g.k[l], 0, 0, g.kbinwidth, L, N);
+                } else {
+                    // host bound of the closing shell's radius: a derived kmax_i/kF is at most
+                    // sqrt(r2hi_i) + sqrt(3)/2 bw (a corner of the selected voxel's cube), and
+                    // k3^2 = a^2 + b^2 - 2ab cos(theta) <= a^2 + b^2 + 2ab max(1, |cos(theta)|)
+                    const Shell s0 = make_shell(SHELL_DEFAULT, g.k[0], 0, 0, g.kbinwidth, L, N);
+                    const Shell s1 = make_shell(SHELL_DEFAULT, g.k[1], 0, 0, g.kbinwidth, L, N);
+                    const double e = 0.8660254037844387 * fabs(g.kbinwidth) + 1e-6;
+                    const double r0 = (s0.r2hi >= 0 ? sqrt((double)s0.r2hi) : 0.0) + e;
+                    const double r1 = (s1.r2hi >= 0 ? sqrt((double)s1.r2hi) : 0.0) + e;
+                    const double cth = (g.k[0] * g.k[0] + g.k[1] * g.k[1] - g.k[2] * g.k[2]) / (2. * g.k[0] * g.k[1]);
+                    const double cmax = std::isfinite(cth) ? std::max(1.0, fabs(cth)) : HUGE_VAL;
+                    const double r3 = sqrt(r0 * r0 + r1 * r1 + 2.0 * r0 * r1 * cmax) * (1.0 + 1e-12);
+                    key.tag = 1;
+                    key.k0 = g.k[0];
+                    key.k1 = g.k[1];
+                    key.k2 = g.k[2];
+                    key.half = 0.5 * g.kbinwidth;
+                    key.sh.kind = SHELL_RANGE;
+                    key.sh.band = band_of(r3 + fabs(0.5 * g.kbinwidth) + 1e-6, N);
+                    key.sh.r2lo = 0;
+                    // upper bound (table sizes only): a full band reaches the corner of the cube
+                    key.sh.r2hi = key.sh.band < N / 2 ? key.sh.band * key.sh.band : 3 * (N / 2) * (N / 2);
+                }
+                break;
+            case PS_BIN_GIVEN:
+                key.sh = last ? make_shell(SHELL_RANGE, 0, g.kmin[l], g.kmax[l], g.kbinwidth, L, N)
+                              : make_shell(SHELL_DEFAULT, g.k[l], 0, 0, g.kbinwidth, L, N);
+                break;
+            case PS_BIN_WATKINSON:
+                key.sh = last ? make_shell(SHELL_WATKINSON_RANGE, 0, g.kmin[l], g.kmax[l], g.kbinwidth, L, N)
+                              : make_shell(SHELL_WATKINSON, g.k[l], 0, 0, g.kbinwidth, L, N);
+                break;
+            default:
+                key.sh = make_shell(SHELL_DEFAULT, g.k[l], 0, 0, g.kbinwidth, L, N);
+                break;
+            }
+            lid[q].push_back(uniq_id(key));
+        }
+        if (g.kbinningCase == PS_BIN_DERIVED) {
+            P->derived_cfgs.push_back(q);
+            const int d0 = derived_slot(make_shell(SHELL_DEFAULT, g.k[0], 0, 0, g.kbinwidth, L, N));
+            const int d1 = derived_slot(make_shell(SHELL_DEFAULT, g.k[1], 0, 0, g.kbinwidth, L, N));
+            ClosingDesc d;
+            memset(&d, 0, sizeof(d));
+            d.cfg = q;
+            d.d0 = d0;
+            d.d1 = d1;
+            d.slot = lid[q][2];
+            d.band = uniq[lid[q][2]].sh.band;
+            d.k0 = g.k[0];
+            d.k1 = g.k[1];
+            d.k2 = g.k[2];
+            d.half = 0.5 * g.kbinwidth;
+            closing.push_back(d);
         }
     }
-    // plan: pair groups (n = 3 sharing a leg pair), n = 2 (Parseval), the rest leg by leg
+    const int nu = (int)uniq.size();
+    auto host_shell_of = [&](int u) -> const Shell& { return uniq[u].sh; };
+
+    // ---- plan: pair groups (n = 3 sharing a leg pair), n = 2 (Parseval), the rest leg by leg
     std::vector<Group> groups;
-    std::vector<int> direct;
-    std::vector<int> pairs2;
+    std::vector<int> direct, pairs2;
     {
         std::map<std::pair<int, int>, int> freq;
         for (int q = 0; q < nconf; q++)
@@ -922,8 +1092,8 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, doubl
                     const int f = freq[{std::min(v[x], v[y]), std::max(v[x], v[y])}];
                     if (f > best) { best = f; bx = x; by = y; }
                 }
-            const int z = 3 - bx - by;
             if (best < 2) { direct.push_back(q); continue; }
+            const int z = 3 - bx - by;
             std::pair<int, int> key{std::min(v[bx], v[by]), std::max(v[bx], v[by])};
             auto it = gidx.find(key);
             if (it == gidx.end()) {
@@ -935,140 +1105,403 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, doubl
             groups[it->second].third.push_back(v[z]);
         }
     }
-    // device scalars: sumD | sumI | coef | scratch D | scratch I | sumA (|terms|) | scratch A
-    PS_TRY(ensure_sums(c, 7 * (size_t)nconf + 4 * MAX_DOT_SHELLS + 8));
-    double* sumD = c->dsums;
-    double* sumI = sumD + nconf;  // exact polygon counts
-    double* dcoef = sumI + nconf;
-    double* gD = dcoef + nconf;
-    double* gI = gD + std::max(nconf, 2 * MAX_DOT_SHELLS);
-    double* sumA = gI + std::max(nconf, 2 * MAX_DOT_SHELLS);
-    double* gA = sumA + nconf;
-    std::vector<double> coef(nconf);
-    for (int q = 0; q < nconf; q++) coef[q] = norm_coef(c->L, N, cfgs[q].n);
-    std::vector<double> hsI_direct;
 
-    // ---- pair groups
+    // ---- shell table: [unique shells][group closing lists][n=2 chunk tables]
+    std::vector<Shell> table(nu);
+    for (int u = 0; u < nu; u++) table[u] = host_shell_of(u);
+    std::vector<int> gofs(groups.size()), copy_src, copy_dst;
+    for (size_t g = 0; g < groups.size(); g++) {
+        gofs[g] = (int)table.size();
+        for (int s : groups[g].third) {
+            if (uniq[s].tag == 1) {  // filled on the device after k_closing
+                copy_src.push_back(s);
+                copy_dst.push_back((int)table.size());
+            }
+            table.push_back(host_shell_of(s));
+        }
+    }
+    struct P2Chunk {
+        int ofs, cnt, band, lut_size, idx_ofs;
+        bool lut_ok;
+    };
+    std::vector<P2Chunk> p2;
+    std::vector<int> idx_all;  // scatter indices (groups, then n=2 chunks)
+    std::vector<int> gidx_ofs(groups.size());
+    for (size_t g = 0; g < groups.size(); g++) {
+        gidx_ofs[g] = (int)idx_all.size();
+        for (int q : groups[g].cfg) idx_all.push_back(q);
+    }
+    for (size_t q0 = 0; q0 < pairs2.size(); q0 += MAX_DOT_SHELLS) {
+        P2Chunk ch;
+        ch.cnt = (int)std::min<size_t>(MAX_DOT_SHELLS, pairs2.size() - q0);
+        ch.ofs = (int)table.size();
+        ch.lut_ok = true;
+        ch.band = 0;
+        ch.lut_size = 0;
+        for (int x = 0; x < ch.cnt; x++) {
+            const Shell& sa = host_shell_of(lid[pairs2[q0 + x]][0]);
+            const Shell& sb = host_shell_of(lid[pairs2[q0 + x]][1]);
+            table.push_back(sa);
+            table.push_back(sb);
+            ch.band = std::max(ch.band, std::min(sa.band, sb.band));
+            if (sa.kind > SHELL_RANGE || sb.kind > SHELL_RANGE) ch.lut_ok = false;
+        }
+        for (int x = 0; x < ch.cnt && ch.lut_ok; x++) {
+            Shell iv = table[ch.ofs + 2 * x];
+            iv.r2lo = std::max(table[ch.ofs + 2 * x].r2lo, table[ch.ofs + 2 * x + 1].r2lo);
+            iv.r2hi = std::min(table[ch.ofs + 2 * x].r2hi, table[ch.ofs + 2 * x + 1].r2hi);
+            ch.lut_size = std::max(ch.lut_size, iv.r2hi + 1);
+            table.push_back(iv);
+        }
+        ch.idx_ofs = (int)idx_all.size();
+        for (int x = 0; x < ch.cnt; x++) idx_all.push_back(pairs2[q0 + x]);
+        p2.push_back(ch);
+    }
+
+    // ---- device buffers of the plan, scratch of the context sized up front
+    Shell* dtable = nullptr;
+    PS_TRY(plan_upload(P, &dtable, table));
+    int* didx = nullptr;
+    PS_TRY(plan_upload(P, &didx, idx_all));
+    int *dcsrc = nullptr, *dcdst = nullptr, *dround = nullptr;
+    PS_TRY(plan_upload(P, &dcsrc, copy_src));
+    PS_TRY(plan_upload(P, &dcdst, copy_dst));
+    PS_TRY(plan_upload(P, &dround, direct));
+    ClosingDesc* dclose = nullptr;
+    PS_TRY(plan_upload(P, &dclose, closing));
+    const int nd = (int)derived.size();
+    Shell* dderived = nullptr;
+    PS_TRY(plan_upload(P, &dderived, derived));
+    std::vector<unsigned long long> mm_init(2 * std::max(nd, 1), 0ull);
+    for (int q = 0; q < nd; q++) memcpy(&mm_init[2 * q], &derived[q].min2_init, 8);
+    unsigned long long *dmm_init = nullptr, *dmm = nullptr;
+    PS_TRY(plan_upload(P, &dmm_init, mm_init));
+    PS_TRY(plan_alloc(P, &dmm, mm_init.size()));
+    double* dkr = nullptr;
+    PS_TRY(plan_alloc(P, &dkr, 2 * (size_t)std::max(nd, 1)));
+    std::vector<double> coef(nconf);
+    for (int q = 0; q < nconf; q++) coef[q] = norm_coef(L, N, cfgs[q].n);
+    double* dcoef = nullptr;
+    PS_TRY(plan_upload(P, &dcoef, coef));
+    const size_t gs = std::max<size_t>(nconf, 2 * MAX_DOT_SHELLS);
+    double *sumD = nullptr, *sumI = nullptr, *sumA = nullptr, *gD = nullptr, *gI = nullptr, *gA = nullptr;
+    PS_TRY(plan_alloc(P, &sumD, nconf));
+    PS_TRY(plan_alloc(P, &sumI, nconf));
+    PS_TRY(plan_alloc(P, &sumA, nconf));
+    PS_TRY(plan_alloc(P, &gD, gs));
+    PS_TRY(plan_alloc(P, &gI, gs));
+    PS_TRY(plan_alloc(P, &gA, gs));
+    PS_TRY(plan_alloc(P, &P->dres, 2 * (size_t)nconf));
+    PS_TRY(plan_alloc(P, &P->dwb, 6 * (size_t)nconf));
+    PS_TRY(plan_alloc(P, &P->derr, 1));
+    PS_CK(cudaMemset(P->derr, 0, sizeof(int)));
+    if (cudaHostAlloc((void**)&P->hres, (10 * (size_t)nconf + 1) * sizeof(double), cudaHostAllocDefault) !=
+        cudaSuccess) {
+        P->hres = nullptr;
+        return fail(PS_ERR_OOM, "pinned result buffer of %d configurations", nconf);
+    }
+    P->dsumA = sumA;
+    P->dsumD = sumD;
     if (!groups.empty()) {
         PS_TRY(ensure_pair_bufs(c, c->f));
         PS_TRY(ensure_pair_bufs(c, c->d));
     }
-    std::vector<Shell> table = uniq;
-    std::vector<int> gofs(groups.size());
-    for (size_t g = 0; g < groups.size(); g++) {
-        gofs[g] = (int)table.size();
-        for (int s : groups[g].third) table.push_back(uniq[s]);
+    {
+        const size_t pen32 = (size_t)N * (c->f.S / pw<float>(N)), pen64 = (size_t)N * (c->d.S / pw<double>(N));
+        PS_TRY(ensure_partials(c, std::max({(size_t)N * N, pen32 * MAX_DOT_SHELLS, pen64 * MAX_DOT_SHELLS,
+                                            (size_t)148 * 8 * 2 * MAX_DOT_SHELLS})));
+        PS_TRY(ensure_lut(c, (size_t)3 * (N / 2) * (N / 2) + 2));
     }
-    PS_TRY(ensure_shells(c, table.size()));
-    PS_CK(cudaMemcpyAsync(c->dshells, table.data(), sizeof(Shell) * table.size(), cudaMemcpyHostToDevice,
-                          c->stream));
+    const double n3 = (double)N * (double)N * (double)N;
+    const double pi = ref_pi();
+    volatile double big = 1.e30;
+    const double min2_init = big * big;
+    P->ops.clear();
+    auto& ops = P->ops;
+
+    // ---- DERIVED chain
+    if (nd > 0) {
+        ops.push_back([=]() {
+            PS_CK(cudaMemcpyAsync(dmm, dmm_init, 16 * (size_t)nd, cudaMemcpyDeviceToDevice, c->stream));
+            for (int q = 0; q < nd; q++) {
+                const int band = std::min(derived[q].band, N / 2);
+                const long long total = (long long)(2 * band + 1) * (2 * band + 1) * (band + 1);
+                const int blocks = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 16));
+                Prof pf(c);
+                k_derived_range<<<blocks, 256, 0, c->stream>>>(N, dderived + q, band, dmm + 2 * q);
+                pf.end(KF_DERIVED, 0.0);
+            }
+            Prof pf(c);
+            k_derive_finish<<<(nd + 127) / 128, 128, 0, c->stream>>>(nd, dmm, pi, L, dkr);
+            pf.end(KF_DERIVED, 0.0);
+            return PS_OK;
+        });
+    }
+    if (!closing.empty()) {
+        const int ncl = (int)closing.size();
+        const int ncp = (int)copy_src.size();
+        int* derr = P->derr;
+        double* dwb = P->dwb;
+        ops.push_back([=]() {
+            Prof pf(c);
+            k_closing<<<(ncl + 127) / 128, 128, 0, c->stream>>>(ncl, dclose, dkr, dtable, dwb, pi, L, N, min2_init,
+                                                                derr);
+            if (ncp > 0) k_copy_shells<<<(ncp + 127) / 128, 128, 0, c->stream>>>(ncp, dcsrc, dcdst, dtable);
+            pf.end(KF_DERIVED, 0.0);
+            return PS_OK;
+        });
+    }
+    // ---- pair groups
     for (size_t g = 0; g < groups.size(); g++) {
-        const Group& G = groups[g];
-        const Shell& sa = uniq[G.a];
-        const Shell& sb = uniq[G.b];
+        const Group G = groups[g];
+        const Shell sa = host_shell_of(G.a), sb = host_shell_of(G.b);
         int hmax = 0;
-        for (int s : G.third) hmax = std::max(hmax, std::min(uniq[s].band, N / 2));
+        for (int s : G.third) hmax = std::max(hmax, std::min(host_shell_of(s).band, N / 2));
         const int hout = hmax + 1;
         const int ng = (int)G.cfg.size();
-        // D part (FP32): P = D_a * D_b formed row by row and transformed back,
-        // then one masked dot product with dk per closing shell
-        int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
-        PS_TRY(c2r_xy<float>(c, LOAD_MASKED, c->dshells + G.a, sa.band, c->f.work, &Sa, &ha));
-        if (G.a != G.b) PS_TRY(c2r_xy<float>(c, LOAD_MASKED, c->dshells + G.b, sb.band, c->f.work2, &Sb, &hbb));
-        PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout, &S));
-        PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gD));
-        if (kappa)
-            PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, c->dshells + gofs[g], table.data() + gofs[g],
-                                   ng, gA));
-        // I part (FP64): the same on unit shells, counts rounded per mode
-        // (unit filters are even in every axis: the xy-quadrant carries everything)
-        PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.a, sa.band, c->d.work, &Sa, &ha, 1));
-        if (G.a != G.b) PS_TRY(c2r_xy<double>(c, LOAD_UNIT, c->dshells + G.b, sb.band, c->d.work2, &Sb, &hbb, 1));
-        PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S, 1));
-        PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, c->dshells + gofs[g], table.data() + gofs[g], ng, gI,
-                                1));
-        PS_TRY(scatter(c, gD, G.cfg, sumD));
-        PS_TRY(scatter(c, gI, G.cfg, sumI));
-        if (kappa) PS_TRY(scatter(c, gA, G.cfg, sumA));
+        const int go = gofs[g], io = gidx_ofs[g];
+        const Shell* hsh = table.data();  // host copy kept alive by the closure below
+        std::vector<Shell> gtable(table.begin() + go, table.begin() + go + ng);
+        ops.push_back([=]() {
+            int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
+            // D part (FP32)
+            PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.a, sa.band, c->f.work, &Sa, &ha));
+            if (G.a != G.b) PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.b, sb.band, c->f.work2, &Sb, &hbb));
+            PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout, &S));
+            PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, dtable + go, gtable.data(), ng, gD));
+            if (kappa)
+                PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, dtable + go, gtable.data(), ng, gA));
+            // I part (FP64 counts on the xy-quadrant: unit filters are even in every axis)
+            PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.a, sa.band, c->d.work, &Sa, &ha, 1));
+            if (G.a != G.b) PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.b, sb.band, c->d.work2, &Sb, &hbb, 1));
+            PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S,
+                                         1));
+            PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, dtable + go, gtable.data(), ng, gI, 1));
+            PS_TRY(scatter_dev(c, gD, didx + io, ng, sumD));
+            PS_TRY(scatter_dev(c, gI, didx + io, ng, sumI));
+            if (kappa) PS_TRY(scatter_dev(c, gA, didx + io, ng, sumA));
+            return PS_OK;
+        });
+        (void)hsh;
     }
-
-    // ---- n = 2 (all terms are |dk|^2 >= 0: condition number 1)
-    if (!pairs2.empty()) PS_TRY(pair2_sums(c, pairs2, lid, uniq, sumD, sumI, gD));
-
+    // ---- n = 2 (Parseval): one k-space pass per chunk
+    for (const P2Chunk ch : p2) {
+        ops.push_back([=]() {
+            const unsigned short* lut = nullptr;
+            if (ch.lut_ok) {
+                Prof pf(c);
+                if (ch.lut_size > 0)
+                    k_shell_lut<<<(ch.lut_size + 255) / 256, 256, 0, c->stream>>>(dtable + ch.ofs + 2 * ch.cnt, ch.cnt,
+                                                                                   ch.lut_size, c->dlut);
+                pf.end(KF_LUT, 2.0 * ch.lut_size);
+                lut = c->dlut;
+            }
+            const int b = std::min(ch.band, N / 2);
+            const long long modes = (long long)(2 * b + 1) * (2 * b + 1) * (b + 1);
+            const int blocks = (int)std::max<long long>(1, std::min<long long>((modes + 255) / 256, 148 * 8));
+            {
+                Prof pf(c);
+                k_pair2_sums<float><<<blocks, 256, 0, c->stream>>>(N, c->f.spec, c->f.S, lut, ch.lut_size, dtable + ch.ofs,
+                                                                   ch.cnt, b, c->partials);
+                pf.end(KF_PAIR2, (double)modes * sizeof(V2<float>));
+            }
+            PS_TRY(sum_partials_n(c, blocks, 2 * MAX_DOT_SHELLS, gD));
+            PS_TRY(scatter_dev(c, gD, didx + ch.idx_ofs, ch.cnt, sumD));
+            PS_TRY(scatter_dev(c, gD + MAX_DOT_SHELLS, didx + ch.idx_ofs, ch.cnt, sumI));
+            return PS_OK;
+        });
+    }
     // ---- leg by leg (singletons, n > 3): running products with powers
-    if (!direct.empty()) {
-        PS_TRY(ensure_shells(c, uniq.size()));
-        PS_CK(cudaMemcpyAsync(c->dshells, uniq.data(), sizeof(Shell) * uniq.size(), cudaMemcpyHostToDevice,
-                              c->stream));
-    }
     for (int q : direct) {
-        const auto& v = lid[q];
         std::vector<std::pair<int, int>> up;  // (shell, multiplicity)
-        for (int s : v) {
+        for (int sidx : lid[q]) {
             bool found = false;
             for (auto& pr : up)
-                if (pr.first == s) { pr.second++; found = true; }
-            if (!found) up.push_back({s, 1});
+                if (pr.first == sidx) { pr.second++; found = true; }
+            if (!found) up.push_back({sidx, 1});
         }
-        const int r = (int)up.size();
-        for (int pass = 0; pass < 2; pass++) {
-            for (int x = 0; x < r; x++) {
-                int epi;
-                if (r == 1) epi = EPI_REDUCE;
-                else epi = x == 0 ? EPI_STORE : (x < r - 1 ? EPI_MUL_STORE : EPI_MUL_REDUCE);
-                const Shell& s = uniq[up[x].first];
-                if (pass == 0) {
-                    PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + up[x].first, s.band, c->f.ra, c->f.ra, epi,
-                                            up[x].second, sumD + q));
-                    if (kappa && x == r - 1)  // |terms| of the same final sum
-                        PS_TRY(c2r_shell<float>(c, LOAD_MASKED, c->dshells + up[x].first, s.band, c->f.ra, c->f.ra,
-                                                r == 1 ? EPI_REDUCE_ABS : EPI_MUL_REDUCE_ABS, up[x].second,
-                                                sumA + q));
-                } else {
-                    PS_TRY(c2r_shell<double>(c, LOAD_UNIT, c->dshells + up[x].first, s.band, c->d.ra, c->d.ra, epi,
-                                             up[x].second, sumI + q));
+        std::vector<int> bands;
+        for (auto& pr : up) bands.push_back(host_shell_of(pr.first).band);
+        ops.push_back([=]() {
+            const int r = (int)up.size();
+            for (int pass = 0; pass < 2; pass++)
+                for (int x = 0; x < r; x++) {
+                    const int epi = r == 1 ? EPI_REDUCE : (x == 0 ? EPI_STORE : (x < r - 1 ? EPI_MUL_STORE : EPI_MUL_REDUCE));
+                    if (pass == 0) {
+                        PS_TRY(c2r_shell<float>(c, LOAD_MASKED, dtable + up[x].first, bands[x], c->f.ra, c->f.ra, epi,
+                                                up[x].second, sumD + q));
+                        if (kappa && x == r - 1)
+                            PS_TRY(c2r_shell<float>(c, LOAD_MASKED, dtable + up[x].first, bands[x], c->f.ra, c->f.ra,
+                                                    r == 1 ? EPI_REDUCE_ABS : EPI_MUL_REDUCE_ABS, up[x].second,
+                                                    sumA + q));
+                    } else {
+                        PS_TRY(c2r_shell<double>(c, LOAD_UNIT, dtable + up[x].first, bands[x], c->d.ra, c->d.ra, epi,
+                                                 up[x].second, sumI + q));
+                    }
                 }
-            }
-        }
+            return PS_OK;
+        });
     }
-    // direct configurations hold grid sums in sumI: convert them to counts
-    // (round(sumI / N^3), exact since the FP64 error is far below 1/2)
-    const double n3 = (double)N * (double)N * (double)N;
     if (!direct.empty()) {
-        std::vector<double> hsI(nconf);
-        PS_CK(cudaMemcpyAsync(hsI.data(), sumI, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream));
-        PS_CK(cudaStreamSynchronize(c->stream));
-        for (int q : direct) hsI[q] = nearbyint(hsI[q] / n3);
-        PS_CK(cudaMemcpyAsync(sumI, hsI.data(), 8 * (size_t)nconf, cudaMemcpyHostToDevice, c->stream));
+        const int nr = (int)direct.size();
+        ops.push_back([=]() {
+            Prof pf(c);
+            k_round_counts<<<(nr + 127) / 128, 128, 0, c->stream>>>(nr, dround, sumI, n3);
+            pf.end(KF_FINAL, 0.0);
+            return PS_OK;
+        });
     }
-    PS_CK(cudaMemcpyAsync(dcoef, coef.data(), 8 * (size_t)nconf, cudaMemcpyHostToDevice, c->stream));
-    double* dout = nullptr;
-    PS_TRY(alloc_dev(&dout, 2 * (size_t)nconf));
-    {
+    double* dres = P->dres;
+    ops.push_back([=]() {
         Prof pf(c);
-        k_finalize<<<(nconf + 127) / 128, 128, 0, c->stream>>>(nconf, dcoef, sumD, sumI, 1.0 / n3, 1, dout);
+        k_finalize<<<(nconf + 127) / 128, 128, 0, c->stream>>>(nconf, dcoef, sumD, sumI, 1.0 / n3, 1, dres);
         pf.end(KF_FINAL, 0.0);
+        PS_CK(cudaGetLastError());
+        return PS_OK;
+    });
+    return PS_OK;
+}
+
+int plan_enqueue(ps_gpu_ctx* c, ps_gpu_plan* P)
+{
+    for (auto& op : P->ops) PS_TRY(op());
+    return PS_OK;
+}
+
+// Results of an executed batched plan: device -> pinned host copy (stream
+// ordered), then unpacked on the host into the caller's arrays.
+int plan_copy_results(ps_gpu_ctx* c, ps_gpu_plan* P)
+{
+    const size_t n = (size_t)P->nconf;
+    double* h = P->hres;
+    PS_CK(cudaMemcpyAsync(h, P->dres, 16 * n, cudaMemcpyDeviceToHost, c->stream));
+    PS_CK(cudaMemcpyAsync(h + 2 * n, P->dwb, 48 * n, cudaMemcpyDeviceToHost, c->stream));
+    if (P->flags & PS_PLAN_KAPPA) {
+        PS_CK(cudaMemcpyAsync(h + 8 * n, P->dsumA, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+        PS_CK(cudaMemcpyAsync(h + 9 * n, P->dsumD, 8 * n, cudaMemcpyDeviceToHost, c->stream));
     }
-    std::vector<double> h(2 * nconf), hA, hD;
-    cudaError_t e1 = cudaMemcpyAsync(h.data(), dout, 16 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream);
-    if (kappa && e1 == cudaSuccess) {
-        hA.resize(nconf);
-        hD.resize(nconf);
-        e1 = cudaMemcpyAsync(hA.data(), sumA, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream);
-        if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(hD.data(), sumD, 8 * (size_t)nconf, cudaMemcpyDeviceToHost, c->stream);
-    }
-    cudaError_t e2 = cudaStreamSynchronize(c->stream);
-    cudaFree(dout);
-    PS_CK(e1);
-    PS_CK(e2);
+    PS_CK(cudaMemcpyAsync(h + 10 * n, P->derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return PS_OK;
+}
+
+// Host side of a finished execution (no CUDA calls: also runs as a stream callback).
+int plan_unpack(const ps_gpu_plan* P, double* B, double* Np, double* kappa, ps_cfg* cfgs_out)
+{
+    const int nconf = P->nconf;
+    const double* h = P->hres;
+    int err = 0;
+    memcpy(&err, h + 10 * (size_t)nconf, sizeof(int));
     for (int q = 0; q < nconf; q++) {
         B[q] = h[2 * q];
         Np[q] = h[2 * q + 1];
+        if (kappa) kappa[q] = P->cfgs[q].n == 2 ? 1.0 : h[8 * (size_t)nconf + q] / fabs(h[9 * (size_t)nconf + q]);
     }
-    if (kappa) {
-        for (int q = 0; q < nconf; q++) kappa[q] = cfgs[q].n == 2 ? 1.0 : hA[q] / fabs(hD[q]);
+    if (cfgs_out) {
+        const double* wb = h + 2 * (size_t)nconf;
+        for (int q = 0; q < nconf; q++) cfgs_out[q] = P->cfgs[q];
+        for (int q : P->derived_cfgs) {
+            for (int l = 0; l < 3; l++) {
+                cfgs_out[q].kmin[l] = wb[6 * q + 2 * l];
+                cfgs_out[q].kmax[l] = wb[6 * q + 2 * l + 1];
+            }
+        }
     }
+    return err ? PS_ERR_CUDA : PS_OK;
+}
+
+int plan_finish(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Np, double* kappa, ps_cfg* cfgs_out)
+{
+    PS_TRY(plan_copy_results(c, P));
+    PS_CK(cudaStreamSynchronize(c->stream));
+    if (plan_unpack(P, B, Np, kappa, cfgs_out) != PS_OK)
+        return fail(PS_ERR_CUDA, "internal: a derived shell exceeded its launch bound");
     return PS_OK;
+}
+
+// An asynchronous submission: unpacked by a host callback in stream order.
+struct SubmitJob {
+    ps_gpu_ctx* c;
+    const ps_gpu_plan* P;
+    double *B, *Np, *kappa;
+    ps_cfg* cfgs_out;
+};
+
+void CUDART_CB submit_callback(void* arg)
+{
+    SubmitJob* j = (SubmitJob*)arg;
+    if (plan_unpack(j->P, j->B, j->Np, j->kappa, j->cfgs_out) != PS_OK) {
+        int expected = 0;
+        j->c->async_err.compare_exchange_strong(expected, PS_ERR_CUDA);
+    }
+    delete j;
+}
+
+// Device and pinned memory of a plan (the plan object itself stays).
+void plan_release(ps_gpu_plan* P)
+{
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    P->exec = nullptr;
+    P->graph = nullptr;
+    for (void* p : P->owned) cudaFree(p);
+    P->owned.clear();
+    if (P->hres) cudaFreeHost(P->hres);
+    P->hres = nullptr;
+    P->ops.clear();
+}
+
+void plan_free(ps_gpu_plan* P)
+{
+    if (!P) return;
+    plan_release(P);
+    delete P;
+}
+
+int plan_run(ps_gpu_ctx* c, ps_gpu_plan* P)
+{
+    if (!(P->flags & PS_PLAN_GRAPH)) return plan_enqueue(c, P);
+    if (!P->exec) {
+        c->capturing = true;
+        const long long before = c->launches;
+        cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            c->capturing = false;
+            return fail(PS_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
+        }
+        const int rc = plan_enqueue(c, P);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(c->stream, &g);
+        c->capturing = false;
+        if (rc != PS_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(PS_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
+        P->graph = g;
+        P->graph_launches = c->launches - before;
+        c->launches = before;
+        PS_CK(cudaGraphInstantiate(&P->exec, P->graph, 0));
+    }
+    PS_CK(cudaGraphLaunch(P->exec, c->stream));
+    c->launches += P->graph_launches;
+    c->launches_total += P->graph_launches;
+    return PS_OK;
+}
+
+int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, double* kappa)
+{
+    if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available (methods mask)");
+    ps_gpu_plan* P = new ps_gpu_plan();
+    P->ctx = c;
+    P->method = PS_FP32_BATCHED;
+    P->nconf = nconf;
+    P->flags = kappa ? PS_PLAN_KAPPA : 0;
+    P->cfgs.assign(cfgs, cfgs + nconf);
+    int rc = plan_batched(c, P);
+    if (rc == PS_OK) rc = plan_enqueue(c, P);
+    if (rc == PS_OK) rc = plan_finish(c, P, B, Np, kappa, cfgs);
+    plan_free(P);
+    return rc;
 }
 
 // =========================================================================
@@ -1188,6 +1621,56 @@ int timed_end(ps_gpu_ctx* c)
     return PS_OK;
 }
 
+// Field load (get_FT_field, input_field.c:40-81) as stream work: host arrays
+// are copied on the copy stream into one of two staging slots, the forward
+// transform waits for that copy on the compute stream, so the upload of the
+// next field overlaps the work still queued on the current one.
+int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int is_double, int mem,
+               int use_only_phase)
+{
+    if (which < PS_FIELD_DENS || which > PS_FIELD_XHI_DENS) return fail(PS_ERR_ARG, "which=%d", which);
+    if (mem != PS_MEM_HOST && mem != PS_MEM_DEVICE) return fail(PS_ERR_ARG, "mem=%d", mem);
+    const void* a = which == PS_FIELD_XHII ? xhii : dens;
+    const void* b = which == PS_FIELD_XHI_DENS ? xhii : nullptr;
+    if (!a || (which == PS_FIELD_XHI_DENS && !b)) return fail(PS_ERR_ARG, "field pointer is NULL");
+    const size_t n3 = (size_t)c->N * c->N * c->N;
+    const size_t bytes = n3 * (is_double ? 8 : 4);
+    int s = -1;
+    if (mem == PS_MEM_HOST) {
+        if (c->stage_bytes < bytes) {
+            // earlier uploads and the transforms reading them finish first
+            PS_CK(cudaStreamSynchronize(c->copy_stream));
+            PS_CK(cudaStreamSynchronize(c->stream));
+            for (int q = 0; q < 2; q++)
+                for (int r = 0; r < 2; r++) {
+                    cudaFree(c->stage[q][r]);
+                    c->stage[q][r] = nullptr;
+                }
+            c->stage_bytes = 0;
+            for (int q = 0; q < 2; q++)
+                for (int r = 0; r < 2; r++) PS_TRY(alloc_dev((unsigned char**)&c->stage[q][r], bytes));
+            c->stage_bytes = bytes;
+        }
+        s = c->slot;
+        c->slot ^= 1;
+        PS_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_free[s], 0));
+        PS_CK(cudaMemcpyAsync(c->stage[s][0], a, bytes, cudaMemcpyHostToDevice, c->copy_stream));
+        if (b) PS_CK(cudaMemcpyAsync(c->stage[s][1], b, bytes, cudaMemcpyHostToDevice, c->copy_stream));
+        PS_CK(cudaEventRecord(c->ev_copied[s], c->copy_stream));
+        PS_CK(cudaStreamWaitEvent(c->stream, c->ev_copied[s], 0));
+        a = c->stage[s][0];
+        if (b) b = c->stage[s][1];
+    }
+    const int kind = b ? (is_double ? SRC_XHI_F64 : SRC_XHI_F32) : (is_double ? SRC_F64 : SRC_F32);
+    c->use_only_phase = use_only_phase;
+    c->f.have_spec = c->d.have_spec = false;
+    if (c->methods & PS_FP32_BATCHED) PS_TRY(forward_field<float>(c, kind, a, b));
+    if (c->methods & PS_FP64_PLAIN) PS_TRY(forward_field<double>(c, kind, a, b));
+    if (s >= 0) PS_CK(cudaEventRecord(c->ev_free[s], c->stream));
+    c->field_set = true;
+    return PS_OK;
+}
+
 }  // namespace
 
 int ps::report_error(int code, const char* msg) { return fail(code, "%s", msg); }
@@ -1249,6 +1732,18 @@ int ps_gpu_create(ps_gpu_ctx** out, int nbins, double boxsize, int methods, int 
             rc = fail(PS_ERR_CUDA, "event creation failed");
             break;
         }
+        if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "stream creation failed");
+            break;
+        }
+        bool ev_ok = true;
+        for (int q = 0; q < 2; q++)
+            ev_ok = ev_ok && cudaEventCreateWithFlags(&c->ev_copied[q], cudaEventDisableTiming) == cudaSuccess &&
+                    cudaEventCreateWithFlags(&c->ev_free[q], cudaEventDisableTiming) == cudaSuccess;
+        if (!ev_ok) {
+            rc = fail(PS_ERR_CUDA, "event creation failed");
+            break;
+        }
         // the batched method transforms shells in FP32 and counts in FP64
         if (methods & PS_FP32_BATCHED) {
             if ((rc = init_prec(c, c->f)) != PS_OK) break;
@@ -1269,38 +1764,19 @@ int ps_gpu_set_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhi
 {
     g_err[0] = 0;
     if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
-    if (which < PS_FIELD_DENS || which > PS_FIELD_XHI_DENS) return fail(PS_ERR_ARG, "which=%d", which);
-    if (mem != PS_MEM_HOST && mem != PS_MEM_DEVICE) return fail(PS_ERR_ARG, "mem=%d", mem);
-    const void* a = which == PS_FIELD_XHII ? xhii : dens;
-    const void* b = which == PS_FIELD_XHI_DENS ? xhii : nullptr;
-    if (!a || (which == PS_FIELD_XHI_DENS && !b)) return fail(PS_ERR_ARG, "field pointer is NULL");
     PS_CK(cudaSetDevice(c->device));
-    const size_t n3 = (size_t)c->N * c->N * c->N;
-    const size_t bytes = n3 * (is_double ? 8 : 4);
     PS_TRY(timed_begin(c));
-    if (mem == PS_MEM_HOST) {
-        if (c->stage_bytes < bytes) {
-            cudaFree(c->stage[0]);
-            cudaFree(c->stage[1]);
-            c->stage[0] = c->stage[1] = nullptr;
-            c->stage_bytes = 0;
-            PS_TRY(alloc_dev((unsigned char**)&c->stage[0], bytes));
-            PS_TRY(alloc_dev((unsigned char**)&c->stage[1], bytes));
-            c->stage_bytes = bytes;
-        }
-        PS_CK(cudaMemcpyAsync(c->stage[0], a, bytes, cudaMemcpyHostToDevice, c->stream));
-        if (b) PS_CK(cudaMemcpyAsync(c->stage[1], b, bytes, cudaMemcpyHostToDevice, c->stream));
-        a = c->stage[0];
-        if (b) b = c->stage[1];
-    }
-    const int kind = b ? (is_double ? SRC_XHI_F64 : SRC_XHI_F32) : (is_double ? SRC_F64 : SRC_F32);
-    c->use_only_phase = use_only_phase;
-    c->f.have_spec = c->d.have_spec = false;
-    if (c->methods & PS_FP32_BATCHED) PS_TRY(forward_field<float>(c, kind, a, b));
-    if (c->methods & PS_FP64_PLAIN) PS_TRY(forward_field<double>(c, kind, a, b));
-    PS_TRY(timed_end(c));
-    c->field_set = true;
-    return PS_OK;
+    PS_TRY(load_field(c, which, dens, xhii, is_double, mem, use_only_phase));
+    return timed_end(c);
+}
+
+int ps_gpu_set_field_async(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int is_double,
+                           int mem, int use_only_phase)
+{
+    g_err[0] = 0;
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    PS_CK(cudaSetDevice(c->device));
+    return load_field(c, which, dens, xhii, is_double, mem, use_only_phase);
 }
 
 int ps_gpu_init(ps_gpu_ctx** ctx, int nbins, double boxsize, const void* field, int field_is_double,
@@ -1495,6 +1971,106 @@ int ps_gpu_last_timing(ps_gpu_ctx* c, double* ms, long long* launches)
     return PS_OK;
 }
 
+int ps_gpu_plan_create(ps_gpu_ctx* c, int method, int nconf, const ps_cfg* cfgs, int flags, ps_gpu_plan** out)
+{
+    g_err[0] = 0;
+    if (!c || !out || (nconf > 0 && !cfgs) || nconf < 0) return fail(PS_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    if (method != PS_FP64_PLAIN && method != PS_FP32_BATCHED) return fail(PS_ERR_ARG, "method %d", method);
+    if (!(c->methods & method)) return fail(PS_ERR_ARG, "method %d not enabled for this context", method);
+    if (flags & ~(PS_PLAN_GRAPH | PS_PLAN_KAPPA)) return fail(PS_ERR_ARG, "flags %d", flags);
+    PS_CK(cudaSetDevice(c->device));
+    ps_gpu_plan* P = new ps_gpu_plan();
+    P->ctx = c;
+    P->method = method;
+    P->nconf = nconf;
+    P->flags = method == PS_FP32_BATCHED ? flags : (flags & PS_PLAN_KAPPA);
+    P->cfgs.assign(cfgs, cfgs + nconf);
+    if (method == PS_FP32_BATCHED && nconf > 0) {
+        const int rc = plan_batched(c, P);
+        if (rc != PS_OK) {
+            plan_free(P);
+            return rc;
+        }
+    }
+    c->plans.insert(P);
+    *out = P;
+    return PS_OK;
+}
+
+int ps_gpu_plan_execute(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly, double* kappa, ps_cfg* cfgs_out)
+{
+    g_err[0] = 0;
+    if (!c || !P || !B || !Npoly) return fail(PS_ERR_ARG, "NULL argument");
+    if (P->ctx != c) return fail(PS_ERR_ARG, "plan belongs to another context");
+    if (!c->field_set) return fail(PS_ERR_ARG, "no field loaded (ps_gpu_set_field)");
+    if (kappa && !(P->flags & PS_PLAN_KAPPA)) return fail(PS_ERR_ARG, "plan created without PS_PLAN_KAPPA");
+    if (P->nconf == 0) return PS_OK;
+    PS_CK(cudaSetDevice(c->device));
+    PS_TRY(timed_begin(c));
+    if (P->method == PS_FP64_PLAIN) {
+        std::vector<ps_cfg> g = P->cfgs;
+        PS_TRY(plain_batch(c, P->nconf, g.data(), B, Npoly, kappa));
+        if (cfgs_out)
+            for (int q = 0; q < P->nconf; q++) cfgs_out[q] = g[q];
+    } else {
+        if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available");
+        if ((P->flags & PS_PLAN_GRAPH) && c->prof_on) PS_TRY(plan_enqueue(c, P));  // profiled: eager
+        else PS_TRY(plan_run(c, P));
+        PS_TRY(plan_finish(c, P, B, Npoly, kappa, cfgs_out));
+    }
+    return timed_end(c);
+}
+
+void ps_gpu_plan_destroy(ps_gpu_plan* P)
+{
+    if (!P) return;
+    if (P->ctx) {
+        cudaSetDevice(P->ctx->device);
+        cudaStreamSynchronize(P->ctx->stream);  // submissions still reading it
+        P->ctx->plans.erase(P);
+    }
+    plan_free(P);
+}
+
+int ps_gpu_plan_submit(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly, double* kappa, ps_cfg* cfgs_out)
+{
+    g_err[0] = 0;
+    if (!c || !P || !B || !Npoly) return fail(PS_ERR_ARG, "NULL argument");
+    if (P->ctx != c) return fail(PS_ERR_ARG, "plan belongs to another context");
+    if (P->method != PS_FP32_BATCHED)
+        return fail(PS_ERR_UNSUPPORTED, "asynchronous submission needs a PS_FP32_BATCHED plan");
+    if (!c->field_set) return fail(PS_ERR_ARG, "no field loaded (ps_gpu_set_field)");
+    if (kappa && !(P->flags & PS_PLAN_KAPPA)) return fail(PS_ERR_ARG, "plan created without PS_PLAN_KAPPA");
+    if (P->nconf == 0) return PS_OK;
+    if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available");
+    PS_CK(cudaSetDevice(c->device));
+    if ((P->flags & PS_PLAN_GRAPH) && c->prof_on) PS_TRY(plan_enqueue(c, P));
+    else PS_TRY(plan_run(c, P));
+    PS_TRY(plan_copy_results(c, P));
+    SubmitJob* j = new SubmitJob{c, P, B, Npoly, kappa, cfgs_out};
+    const cudaError_t e = cudaLaunchHostFunc(c->stream, submit_callback, j);
+    if (e != cudaSuccess) {
+        delete j;
+        return fail(PS_ERR_CUDA, "cudaLaunchHostFunc: %s", cudaGetErrorString(e));
+    }
+    return PS_OK;
+}
+
+int ps_gpu_synchronize(ps_gpu_ctx* c)
+{
+    g_err[0] = 0;
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    PS_CK(cudaSetDevice(c->device));
+    PS_CK(cudaStreamSynchronize(c->copy_stream));
+    PS_CK(cudaStreamSynchronize(c->stream));
+    const int e = c->async_err.exchange(0);
+    if (e != PS_OK) return fail(e, "internal: a derived shell exceeded its launch bound (asynchronous execution)");
+    return PS_OK;
+}
+
+long long ps_gpu_launch_count(ps_gpu_ctx* c) { return c ? c->launches_total : -1; }
+
 int ps_gpu_set_profiling(ps_gpu_ctx* c, int on)
 {
     if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
@@ -1534,6 +2110,12 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    for (ps_gpu_plan* P : c->plans) {  // plans outliving their context keep only their host part
+        plan_release(P);
+        P->ctx = nullptr;
+    }
+    c->plans.clear();
     free_prec(c->f);
     free_prec(c->d);
     cudaFree(c->partials);
@@ -1541,9 +2123,13 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     cudaFree(c->dshells);
     cudaFree(c->dminmax);
     cudaFree(c->dlut);
-    cudaFree(c->didx);
-    cudaFree(c->stage[0]);
-    cudaFree(c->stage[1]);
+    for (void* p : c->retired) cudaFree(p);
+    for (int q = 0; q < 2; q++) {
+        for (int r = 0; r < 2; r++) cudaFree(c->stage[q][r]);
+        if (c->ev_copied[q]) cudaEventDestroy(c->ev_copied[q]);
+        if (c->ev_free[q]) cudaEventDestroy(c->ev_free[q]);
+    }
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

@@ -178,3 +178,95 @@ def test_power_spectrum_sweep_many_shells(gpu_lib, ora):
         ref, got = run_both(ps, ora, n_grid, box, case, method)
         assert len(got.k) == n_grid // 2
         check(ref, got, method, f"pk m={method}")
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+def test_plan_replay_matches_batch(gpu_lib, graph):
+    """A plan (optionally captured into a CUDA graph on first execution)
+    executed on two different fields gives, on each, exactly what an eager
+    batch gives, including the DERIVED write-back."""
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    d1, x1 = fields(n_grid, box)
+    d2, x2 = fields(n_grid, box, seed=7)
+    cfgs = []
+    for k1, k2 in ((0.1, 0.14), (0.12, 0.2)):
+        c, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1, k2=k2, num_values=5, kbinningCase=1)
+        cfgs += [c[i] for i in range(len(c))]
+    eq, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, equilateral=1, num_values=3)
+    p2, _, _ = ps.read_params_to_kvectors(n_grid, box, 2, num_values=2)
+    cfgs += [eq[i] for i in range(len(eq))] + [p2[i] for i in range(len(p2))]
+    with ps.Context(n_grid, box) as ctx:
+        plan = ctx.plan(cfgs, graph=graph, kappa=True)
+        for dens, xhii in ((d1, x1), (d2, x2), (d1, x1)):
+            dd, xx = field_args(2, dens, xhii)
+            ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+            Bp, Np, kp, out = plan.execute()
+            Be, Ne, ke, arr = ctx.batch(cfgs, ps.PS_FP32_BATCHED, kappa=True)
+            np.testing.assert_array_equal(Bp, Be)
+            np.testing.assert_array_equal(Np, Ne)
+            np.testing.assert_array_equal(kp, ke)
+            for i in range(len(cfgs)):
+                assert list(out[i].kmin)[:3] == list(arr[i].kmin)[:3]
+                assert list(out[i].kmax)[:3] == list(arr[i].kmax)[:3]
+        plan.close()
+
+
+@pytest.mark.parametrize("pinned", [False, True], ids=["pageable", "pinned"])
+def test_async_pipeline_matches_sync(gpu_lib, pinned):
+    """Fields uploaded with set_field_async and plans submitted without waiting
+    (uploads of the next field overlapping the current configurations) give,
+    per field, exactly the synchronous results, DERIVED write-back and
+    condition numbers included."""
+    import torch
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    flds = [fields(n_grid, box), fields(n_grid, box, seed=7), fields(n_grid, box, seed=11)]
+    cfgs = []
+    for k1, k2 in ((0.1, 0.14), (0.12, 0.2)):
+        c, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1, k2=k2, num_values=5, kbinningCase=1)
+        cfgs += [c[i] for i in range(len(c))]
+    p2, _, _ = ps.read_params_to_kvectors(n_grid, box, 2, num_values=2)
+    cfgs += [p2[i] for i in range(len(p2))]
+    args = []
+    for dens, xhii in flds:
+        dd, xx = field_args(2, dens, xhii)
+        if pinned:
+            dd, xx = torch.from_numpy(dd).pin_memory(), torch.from_numpy(xx).pin_memory()
+        args.append((dd, xx))
+    with ps.Context(n_grid, box, methods=ps.PS_FP32_BATCHED) as ctx:
+        plan = ctx.plan(cfgs, graph=True, kappa=True)
+        want = []
+        for dd, xx in args:
+            ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+            want.append(plan.execute())
+        subs = []
+        order = [0, 1, 2, 1, 0, 2]
+        for f in order:
+            ctx.set_field_async(2, *args[f], use_only_phase=1)
+            subs.append(plan.submit())
+        ctx.synchronize()
+        for f, sub in zip(order, subs):
+            B, Np, kap, out = want[f]
+            np.testing.assert_array_equal(sub.B, B)
+            np.testing.assert_array_equal(sub.npoly, Np)
+            np.testing.assert_array_equal(sub.kappa, kap)
+            for i in range(len(cfgs)):
+                assert list(sub.cfgs[i].kmin)[:3] == list(out[i].kmin)[:3]
+                assert list(sub.cfgs[i].kmax)[:3] == list(out[i].kmax)[:3]
+        plan.close()
+
+
+def test_plan_outliving_context(gpu_lib):
+    """Closing the context first leaves the plan destroyable and unusable."""
+    ps = gpu_lib
+    ctx = ps.Context(16, 100.0)
+    ctx.get_FT_field(0, fields(16, 100.0)[0])
+    cfgs, _, _ = ps.read_params_to_kvectors(16, 100.0, 3, k1=0.2, k2=0.3, num_values=3)
+    plan = ctx.plan(cfgs)
+    plan.execute()
+    n0 = ctx.launch_count()
+    plan.execute()
+    assert ctx.launch_count() > n0
+    ctx.close()
+    plan.close()
