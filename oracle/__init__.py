@@ -25,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libps_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libpsref.so")
+REF_EXE = os.path.join(HERE, "_ref", "polyspectrum")  # the reference's own executable (main.c)
 
 FIELD_NAMES = {0: "DENS", 1: "XHII", 2: "XHI_DENS"}
 BINNING_NAMES = {0: "DEFAULT", 1: "DERIVED_BINNING", 2: "GIVEN_BINNING", 3: "WATKINSON"}
@@ -251,6 +252,15 @@ _ref = None
 
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+def ref_exe_available() -> bool:
+    return os.path.exists(REF_EXE)
+
+
+def run_ref_exe(ini_path: str, cwd: str | None = None, timeout: float = 600.0) -> subprocess.CompletedProcess:
+    """Run the reference executable on an ini file (serial build, shim FFT)."""
+    return subprocess.run([REF_EXE, ini_path], cwd=cwd, capture_output=True, text=True, timeout=timeout)
 
 
 def ref_lib() -> C.CDLL:

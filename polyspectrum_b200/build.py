@@ -5,7 +5,9 @@
 Each translation unit compiles in its own nvcc process (the FFT kernels are
 heavily unrolled); objects go to polyspectrum_b200/_build/, the shared library
 to polyspectrum_b200/libpsgpu.so.  The library links the CUDA runtime
-statically and depends on no torch symbol.
+statically and depends on no torch symbol.  The command-line driver
+(driver/ps_run.c, plain C over the C-ABI) is linked against it as
+polyspectrum_b200/ps_run.
 """
 from __future__ import annotations
 
@@ -21,6 +23,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libpsgpu.so")
+DRIVER_SRC = os.path.join(PKG, "driver", "ps_run.c")
+DRIVER = os.path.join(PKG, "ps_run")
 SOURCES = ["ps_api.cu", "ps_inst_f32.cu", "ps_inst_f64.cu", "ps_noalloc.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -46,8 +50,22 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in _deps())
 
 
+def build_driver(force: bool = False) -> str:
+    """gcc the C driver against libpsgpu.so (rpath $ORIGIN: the two stay side by side)."""
+    if (not force and os.path.exists(DRIVER)
+            and os.path.getmtime(DRIVER) >= max(os.path.getmtime(DRIVER_SRC), os.path.getmtime(LIB),
+                                                os.path.getmtime(os.path.join(ROOT, "include", "ps_gpu.h")))):
+        return DRIVER
+    tmp = DRIVER + ".tmp"
+    subprocess.run(["gcc", "-std=c99", "-O2", "-Wall", "-Wextra", "-o", tmp, DRIVER_SRC, "-L", PKG, "-lpsgpu",
+                    "-Wl,-rpath,$ORIGIN", "-lm"], check=True)
+    os.replace(tmp, DRIVER)
+    return DRIVER
+
+
 def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = False) -> str:
     if not force and up_to_date():
+        build_driver()
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     exe = nvcc()
@@ -76,6 +94,7 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = False)
     tmp = LIB + ".tmp"
     subprocess.run([exe, *ARCH, "-shared", "-cudart", "static", *objs, "-o", tmp], check=True)
     os.replace(tmp, LIB)
+    build_driver(force=True)
     return LIB
 
 
