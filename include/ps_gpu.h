@@ -205,7 +205,8 @@ int ps_gpu_last_timing(ps_gpu_ctx *ctx, double *ms, long long *kernel_launches);
 /* Per-kernel device timing.  When profiling is on, every kernel the context
  * launches is bracketed by CUDA events on the context's stream and charged,
  * with its algorithmic HBM bytes (the bytes its pass must read and write at
- * minimum), to its kernel family.  ps_gpu_kernel_stats synchronises and
+ * minimum), to its kernel family (FP64 instances of the transform kernels
+ * as "<family>_f64").  ps_gpu_kernel_stats synchronises and
  * returns up to max families; the counters reset when profiling is switched
  * on.  No reference counterpart (the reference has only a total wall time,
  * main.c:38-82). */

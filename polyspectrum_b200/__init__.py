@@ -286,8 +286,8 @@ class Context:
 
     def kernel_stats(self) -> list[dict]:
         """Per kernel family: launches, summed device ms, summed algorithmic bytes."""
-        buf = (ps_kernel_stat * 16)()
-        cnt = _check(lib().ps_gpu_kernel_stats(self._h, buf, 16))
+        buf = (ps_kernel_stat * 64)()
+        cnt = min(_check(lib().ps_gpu_kernel_stats(self._h, buf, 64)), 64)
         return [dict(name=buf[i].name.decode(), launches=buf[i].launches, ms=buf[i].ms,
                      bytes=buf[i].bytes) for i in range(cnt)]
 

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <functional>
 #include <map>
@@ -83,6 +84,8 @@ template <typename T> struct PrecBufs {
     T* rb = nullptr;
     int S = 0;
     bool have_spec = false;
+    // tables of smaller transform sizes (sub-grid products), made at plan time
+    std::map<int, std::array<V2<T>*, 3>> sub;
 };
 
 struct ps_gpu_ctx {
@@ -133,9 +136,9 @@ struct ps_gpu_ctx {
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
-    double prof_ms[16] = {0};
-    double prof_bytes[16] = {0};
-    long long prof_n[16] = {0};
+    double prof_ms[32] = {0};
+    double prof_bytes[32] = {0};
+    long long prof_n[32] = {0};
 };
 
 namespace {
@@ -200,8 +203,52 @@ template <typename T> int init_prec(ps_gpu_ctx* c, PrecBufs<T>& b)
     return PS_OK;
 }
 
+template <typename T> PrecBufs<T>& bufs(ps_gpu_ctx* c);
+
+// Twiddle tables of an M-point transform (M <= N): the context's own for M = N,
+// else made once (allocation: plan time only, never during graph capture).
+template <typename T> int tables_for(ps_gpu_ctx* c, int M, Tables<T>* out)
+{
+    PrecBufs<T>& b = bufs<T>(c);
+    if (M == c->N) {
+        *out = b.tables();
+        return PS_OK;
+    }
+    auto it = b.sub.find(M);
+    if (it == b.sub.end()) {
+        if (c->capturing) return fail(PS_ERR_ARG, "internal: tables of size %d not made before capture", M);
+        std::array<V2<T>*, 3> t = {nullptr, nullptr, nullptr};
+        std::vector<V2<T>> hp(M), hr(M / 2), h(M);
+        const int N = M;
+        PS_SWITCH_N(N, (L3<T, NN>::host_tables(hp.data(), hr.data())));
+        const long double two_pi = 6.283185307179586476925286766559005768L;
+        for (int m = 0; m < M; m++) {
+            const long double a = two_pi * (long double)m / (long double)M;
+            h[m].x = (T)cosl(a);
+            h[m].y = (T)(-sinl(a));
+        }
+        int rc = alloc_dev(&t[0], M);
+        if (rc == PS_OK) rc = alloc_dev(&t[1], M / 2);
+        if (rc == PS_OK) rc = alloc_dev(&t[2], M);
+        if (rc != PS_OK) {
+            for (V2<T>* p : t) cudaFree(p);
+            return rc;
+        }
+        b.sub[M] = t;
+        PS_CK(cudaMemcpy(t[0], hp.data(), sizeof(V2<T>) * M, cudaMemcpyHostToDevice));
+        PS_CK(cudaMemcpy(t[1], hr.data(), sizeof(V2<T>) * (M / 2), cudaMemcpyHostToDevice));
+        PS_CK(cudaMemcpy(t[2], h.data(), sizeof(V2<T>) * M, cudaMemcpyHostToDevice));
+        it = b.sub.find(M);
+    }
+    *out = Tables<T>{it->second[0], it->second[1], it->second[2]};
+    return PS_OK;
+}
+
 template <typename T> void free_prec(PrecBufs<T>& b)
 {
+    for (auto& kv : b.sub)
+        for (V2<T>* p : kv.second) cudaFree(p);
+    b.sub.clear();
     cudaFree(b.tw);
     cudaFree(b.twp);
     cudaFree(b.twr);
@@ -300,6 +347,9 @@ const char* const kFamilyName[KF_COUNT] = {"fwd_z_r2c", "pass_y", "fwd_x_store",
                                            "inv_x_masked", "inv_z_c2r", "sum_partials",
                                            "derived_range", "finalize", "pair_z", "shell_lut", "adjoint",
                                            "pair2_parseval"};
+// families of FP64 transform kernels are counted apart (name suffix _f64)
+constexpr int KF_SLOTS = 2 * KF_COUNT;
+template <typename T> constexpr int fam(int kind) { return sizeof(T) == 8 ? kind + KF_COUNT : kind; }
 
 int prof_fold(ps_gpu_ctx* c)
 {
@@ -361,28 +411,32 @@ int sum_partials(ps_gpu_ctx* c, int nblocks, int ncols, double* out, int out_str
 
 // Inverse X and Y passes of a shell-filtered spectrum into dst, band-limited to
 // the shell: h < hb = min(band, N/2) + 1 columns, row stride *S_out.
-// mode: LOAD_MASKED (F * field spectrum) or LOAD_UNIT (F).
+// mode: LOAD_MASKED (F * field spectrum) or LOAD_UNIT (F).  M > 0 runs the
+// transform on an M-grid (M < N, the shell's band below M/2): the same
+// spectrum sampled on a coarser real-space grid.
 template <typename T>
 int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, int* S_out, int* hb_out,
-           int quad = 0)
+           int quad = 0, int M = 0)
 {
     PrecBufs<T>& B = bufs<T>(c);
-    const int N = c->N;
+    const int N = M > 0 ? M : c->N;
+    Tables<T> tb;
+    PS_TRY(tables_for<T>(c, N, &tb));
     const int hb = std::min(band, N / 2) + 1;
     const int S = round_up(hb, pw<T>(N));
     const double V = sizeof(V2<T>), NN2 = (double)N * N;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, dst, S, mode, dshell, N / 2 + 1, B.tables(),
-                                                quad))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, dst, S, mode, dshell, N / 2 + 1, tb, quad,
+                                                c->N))));
         const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
-        pf.end(KF_INV_X, q * NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
+        pf.end(fam<T>(KF_INV_X), q * NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, B.tables(), quad))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, tb, quad))));
         const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
-        pf.end(KF_PASS_Y, 2.0 * q * NN2 * S * V);
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V);
     }
     *S_out = S;
     *hb_out = hb;
@@ -409,7 +463,7 @@ int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, co
         const double real = NN2 * N * sizeof(T);
         const double extra = (epi == EPI_STORE ? real : 0.0) + (epi == EPI_MUL_STORE ? 2.0 * real : 0.0) +
                              (epi == EPI_MUL_REDUCE ? real : 0.0);
-        pf.end(KF_INV_Z, NN2 * hb * V + extra);
+        pf.end(fam<T>(KF_INV_Z), NN2 * hb * V + extra);
     }
     if (reduce) PS_TRY(sum_partials(c, nb, 1, dsum, 1));
     PS_CK(cudaGetLastError());
@@ -418,25 +472,27 @@ int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, co
 
 // Spectrum of the real product of two band-limited inverse transforms (B may be
 // NULL: square of A), rows kept to h < hout, forward Y pass done; into B.work3.
+// M > 0: the inputs are M-grid transforms (c2r_xy with the same M).
 template <typename T>
 int pair_spectrum(ps_gpu_ctx* c, const V2<T>* A, int Sa, int hba, const V2<T>* Bq, int Sb, int hbb, int hout,
-                  int* S_out, int quad = 0)
+                  int* S_out, int quad = 0, int M = 0)
 {
     PrecBufs<T>& B = bufs<T>(c);
-    const int N = c->N;
+    const int N = M > 0 ? M : c->N;
+    Tables<T> tb;
+    PS_TRY(tables_for<T>(c, N, &tb));
     const int S = round_up(hout, pw<T>(N));
     const double V = sizeof(V2<T>), NN2 = (double)N * N;
     const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, B.tables(),
-                                                 quad))));
-        pf.end(KF_PAIR_Z, q * NN2 * (hba + (Bq ? hbb : 0) + hout) * V);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, tb, quad))));
+        pf.end(fam<T>(KF_PAIR_Z), q * NN2 * (hba + (Bq ? hbb : 0) + hout) * V);
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, B.tables(), quad))));
-        pf.end(KF_PASS_Y, 2.0 * q * NN2 * S * V);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, tb, quad))));
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V);
     }
     *S_out = S;
     return PS_OK;
@@ -455,12 +511,12 @@ int r2c_work(ps_gpu_ctx* c, int kind, const void* a, const void* b, int hout, in
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.work, S, hout, B.tables()))));
-        pf.end(KF_FWD_Z, NN2 * N * src_bytes + NN2 * hout * V);
+        pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * hout * V);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, false, B.tables()))));
-        pf.end(KF_PASS_Y, 2.0 * NN2 * S * V);
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * S * V);
     }
     *stride_out = S;
     return PS_OK;
@@ -477,18 +533,18 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, N / 2 + 1, B.tables()))));
-        pf.end(KF_FWD_Z, NN2 * N * src_bytes + NN2 * H * V);
+        pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * H * V);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tables()))));
-        pf.end(KF_PASS_Y, 2.0 * NN2 * B.S * V);
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * B.S * V);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.spec, B.S, N / 2 + 1, epi, B.spec, B.S, nullptr, 0,
                                                 nullptr, 0, nullptr, 0, nullptr, B.tables(), nullptr))));
-        pf.end(KF_FWD_X_STORE, 2.0 * NN2 * H * V);
+        pf.end(fam<T>(KF_FWD_X_STORE), 2.0 * NN2 * H * V);
     }
     PS_CK(cudaGetLastError());
     B.have_spec = true;
@@ -498,12 +554,15 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
 // Dot / count pass over a forward-transformed work buffer (stride S, band
 // hvalid) for up to MAX_DOT_SHELLS shells per launch; results to dout[0..ns).
 // hsh: host copies of the shells (decide whether an r2 bitmask table applies).
+// M > 0: the buffer is an M-grid spectrum; dot sums are scaled by `weight`.
 template <typename T>
 int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell* dshells,
-             const Shell* hsh, int ns, double* dout, int quad = 0)
+             const Shell* hsh, int ns, double* dout, int quad = 0, int M = 0, double weight = 1.0)
 {
     PrecBufs<T>& B = bufs<T>(c);
-    const int N = c->N;
+    const int N = M > 0 ? M : c->N;
+    Tables<T> tb;
+    PS_TRY(tables_for<T>(c, N, &tb));
     for (int s0 = 0; s0 < ns; s0 += MAX_DOT_SHELLS) {
         const int cnt = std::min(MAX_DOT_SHELLS, ns - s0);
         const size_t blocks = (size_t)N * (S / pw<T>(N));
@@ -527,10 +586,10 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
         {
             Prof pf(c);
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, data, S, hvalid, epi, nullptr, 0, B.spec, B.S,
-                                                    dshells + s0, cnt, lut, lut_size, c->partials, B.tables(), &nb,
-                                                    1.0, quad))));
+                                                    dshells + s0, cnt, lut, lut_size, c->partials, tb, &nb,
+                                                    weight, quad, c->N))));
             const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / ((double)N * N) : 1.0;
-            pf.end(KF_FWD_X_DOT, q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
+            pf.end(fam<T>(KF_FWD_X_DOT), q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
         }
         PS_TRY(sum_partials(c, nb, cnt, dout + s0, 1));
     }
@@ -954,6 +1013,21 @@ struct LegKey {
     }
 };
 
+// Smallest transform size M (a power of two, 16 <= M <= N) on which a pair
+// group with leg bands ba, bb (largest |component| of a mode) and closing
+// bands up to bc runs alias-free.  A triple m_a + m_b + m_c = 0 (mod M) with
+// each component of |m_i| <= b_i and b_a + b_b + b_c < M is zero outright, so
+// the cyclic sums over the M-grid and over the N-grid count the same triples
+// (the reference's N-grid sums then have no aliased triples either); 2 b < M
+// keeps every mode of a shell on its own M-grid index.  N when none fits.
+int alias_free_grid(int N, int ba, int bb, int bc)
+{
+    const int bmax = std::max({ba, bb, bc});
+    for (int M = 16; M < N; M *= 2)
+        if (M > ba + bb + bc && M > 2 * bmax) return M;
+    return N;
+}
+
 int sum_partials_n(ps_gpu_ctx* c, int nblocks, int ncols, double* out)
 {
     return sum_partials(c, nblocks, ncols, out, 1);
@@ -1262,21 +1336,35 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         const int go = gofs[g], io = gidx_ofs[g];
         const Shell* hsh = table.data();  // host copy kept alive by the closure below
         std::vector<Shell> gtable(table.begin() + go, table.begin() + go + ng);
+        // the group's transforms run on the smallest M-grid on which no triple
+        // of its modes aliases (scale of the product spectrum: (N/M)^3)
+        const int M = alias_free_grid(N, std::min(sa.band, N / 2), std::min(sb.band, N / 2), hmax);
+        const double wD = ((double)N / M) * ((double)N / M) * ((double)N / M);
+        if (M < N) {
+            Tables<float> t32;
+            Tables<double> t64;
+            PS_TRY(tables_for<float>(c, M, &t32));
+            PS_TRY(tables_for<double>(c, M, &t64));
+        }
         ops.push_back([=]() {
             int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
             // D part (FP32)
-            PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.a, sa.band, c->f.work, &Sa, &ha));
-            if (G.a != G.b) PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.b, sb.band, c->f.work2, &Sb, &hbb));
-            PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout, &S));
-            PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, dtable + go, gtable.data(), ng, gD));
+            PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.a, sa.band, c->f.work, &Sa, &ha, 0, M));
+            if (G.a != G.b)
+                PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.b, sb.band, c->f.work2, &Sb, &hbb, 0, M));
+            PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout, &S,
+                                        0, M));
+            PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, dtable + go, gtable.data(), ng, gD, 0, M, wD));
             if (kappa)
-                PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, dtable + go, gtable.data(), ng, gA));
+                PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, dtable + go, gtable.data(), ng, gA, 0,
+                                       M, wD));
             // I part (FP64 counts on the xy-quadrant: unit filters are even in every axis)
-            PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.a, sa.band, c->d.work, &Sa, &ha, 1));
-            if (G.a != G.b) PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.b, sb.band, c->d.work2, &Sb, &hbb, 1));
+            PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.a, sa.band, c->d.work, &Sa, &ha, 1, M));
+            if (G.a != G.b)
+                PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.b, sb.band, c->d.work2, &Sb, &hbb, 1, M));
             PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S,
-                                         1));
-            PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, dtable + go, gtable.data(), ng, gI, 1));
+                                         1, M));
+            PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, dtable + go, gtable.data(), ng, gI, 1, M));
             PS_TRY(scatter_dev(c, gD, didx + io, ng, sumD));
             PS_TRY(scatter_dev(c, gI, didx + io, ng, sumI));
             if (kappa) PS_TRY(scatter_dev(c, gA, didx + io, ng, sumA));
@@ -1525,7 +1613,7 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
     if (n == 2) {
         Prof pf(c);
         k_grad_pair2<T><<<148 * 8, 256, 0, c->stream>>>(N, B.spec, B.S, c->dshells, B.hacc, B.S, hb);
-        pf.end(KF_GRAD, 2.0 * N * N * hb * sizeof(V2<T>));
+        pf.end(fam<T>(KF_GRAD), 2.0 * N * N * hb * sizeof(V2<T>));
     } else {
         // leg i: FFT of the product of the other two legs, masked by F_i;
         // identical (mask, pair) terms are folded into one with a weight
@@ -1558,7 +1646,7 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.work3, S, hout, SPEC_MASK_ADD, B.hacc, B.S, nullptr,
                                                     0, c->dshells + li, 1, nullptr, 0, nullptr, B.tables(),
                                                     nullptr, (double)tm.second))));
-            pf.end(KF_GRAD, 3.0 * N * N * S * sizeof(V2<T>));
+            pf.end(fam<T>(KF_GRAD), 3.0 * N * N * S * sizeof(V2<T>));
         }
     }
     // inverse transform of the accumulated spectrum into B.ra, then scale
@@ -1567,18 +1655,18 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.hacc, B.S, B.work, S, LOAD_PLAIN, nullptr, hb, B.tables()))));
-        pf.end(KF_INV_X, 2.0 * N * N * S * sizeof(V2<T>));
+        pf.end(fam<T>(KF_INV_X), 2.0 * N * N * S * sizeof(V2<T>));
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, true, B.tables()))));
-        pf.end(KF_PASS_Y, 2.0 * N * N * S * sizeof(V2<T>));
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * N * N * S * sizeof(V2<T>));
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_z(c->stream, B.work, S, hb, B.ra, nullptr, EPI_STORE, 1, nullptr,
                                                 B.tables(), &nb))));
-        pf.end(KF_INV_Z, (double)N * N * hb * sizeof(V2<T>) + (double)n3 * sizeof(T));
+        pf.end(fam<T>(KF_INV_Z), (double)N * N * hb * sizeof(V2<T>) + (double)n3 * sizeof(T));
     }
     void* dst = out;
     void* stage = nullptr;
@@ -1593,7 +1681,7 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
             k_scale_out<T, double><<<148 * 8, 256, 0, c->stream>>>(B.ra, (double*)dst, n3, scale);
         else
             k_scale_out<T, float><<<148 * 8, 256, 0, c->stream>>>(B.ra, (float*)dst, n3, scale);
-        pf.end(KF_GRAD, (double)n3 * (sizeof(T) + (out_is_double ? 8 : 4)));
+        pf.end(fam<T>(KF_GRAD), (double)n3 * (sizeof(T) + (out_is_double ? 8 : 4)));
     }
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && stage) {
@@ -2076,7 +2164,7 @@ int ps_gpu_set_profiling(ps_gpu_ctx* c, int on)
     if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
     PS_TRY(prof_fold(c));
     if (on && !c->prof_on) {
-        for (int q = 0; q < 16; q++) {
+        for (int q = 0; q < KF_SLOTS; q++) {
             c->prof_ms[q] = c->prof_bytes[q] = 0.0;
             c->prof_n[q] = 0;
         }
@@ -2091,11 +2179,12 @@ int ps_gpu_kernel_stats(ps_gpu_ctx* c, ps_kernel_stat* out, int max)
     PS_CK(cudaSetDevice(c->device));
     PS_TRY(prof_fold(c));
     int cnt = 0;
-    for (int q = 0; q < KF_COUNT; q++) {
+    for (int q = 0; q < KF_SLOTS; q++) {
         if (!c->prof_n[q]) continue;
         if (out && cnt < max) {
             memset(&out[cnt], 0, sizeof(ps_kernel_stat));
-            snprintf(out[cnt].name, sizeof(out[cnt].name), "%s", kFamilyName[q]);
+            snprintf(out[cnt].name, sizeof(out[cnt].name), "%s%s", kFamilyName[q % KF_COUNT],
+                     q >= KF_COUNT ? "_f64" : "");
             out[cnt].launches = c->prof_n[q];
             out[cnt].ms = c->prof_ms[q];
             out[cnt].bytes = c->prof_bytes[q];

@@ -137,7 +137,7 @@ enum InvLoad : int { LOAD_PLAIN = 0, LOAD_MASKED = 1, LOAD_UNIT = 2 };
 
 template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
-    k_inv_x(const V2<T>* __restrict__ src, int src_stride, V2<T>* __restrict__ dst, int dst_stride,
+    k_inv_x(const V2<T>* __restrict__ src, int src_stride, int nsrc, V2<T>* __restrict__ dst, int dst_stride,
             int mode, const Shell* __restrict__ shell_p, int hvalid, int quad, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
@@ -149,13 +149,17 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
     const int tiles_per_row = dst_stride / G::W;
     // quad: pencils j <= N/2 only, outputs i <= N/2 only, stored [i][j][h] with
-    // N/2+1 rows per plane (the unit filter is even in every axis)
+    // N/2+1 rows per plane (the unit filter is even in every axis).
+    // nsrc: grid size of the source spectrum ([nsrc][nsrc][src_stride]); a mode
+    // m of this N-grid is read at index m mod nsrc there (nsrc >= N, and the
+    // shell's band is below N/2, so every selected mode has one home in both).
     const int nj = quad ? N / 2 + 1 : N;
     const int j = blockIdx.x / tiles_per_row;
     const int h = (blockIdx.x % tiles_per_row) * G::W + w;
     const int my = lattice_freq(j, N);
     const int mz = h == N / 2 ? -(N / 2) : h;
     const bool col_ok = h < hvalid && h <= N / 2;
+    const size_t js = (size_t)(my < 0 ? my + nsrc : my);
     Shell sh;
     if (mode != LOAD_PLAIN) sh = *shell_p;
     const bool pencil_live =
@@ -176,11 +180,11 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     V a[G::R];
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
-        const int i = t + G::TPF * e;
+        const int mx = lattice_freq(t + G::TPF * e, N);
         V v = czero<V>();
         if ((bits >> e) & 1u) {
             if (mode == LOAD_UNIT) v = V{(T)1, (T)0};
-            else v = src[((size_t)i * N + j) * src_stride + h];
+            else v = src[((size_t)(mx < 0 ? mx + nsrc : mx) * nsrc + js) * src_stride + h];
         }
         a[e] = v;
     }
@@ -515,7 +519,7 @@ enum SpecEpi : int {
 template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
-            const V2<T>* __restrict__ dk, int dk_stride, const Shell* __restrict__ shells,
+            const V2<T>* __restrict__ dk, int dk_stride, int ndk, const Shell* __restrict__ shells,
             int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight, int quad,
             double* __restrict__ partials, const V2<T>* __restrict__ tw_g)
 {
@@ -532,6 +536,9 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     const bool col_ok = h < hvalid && h <= N / 2;
     const int my = lattice_freq(j, N);
     const int mz = h == N / 2 ? -(N / 2) : h;
+    // dk: field spectrum of an ndk-grid ([ndk][ndk][dk_stride], ndk >= N); mode m
+    // of this grid sits at index m mod ndk there (the shells lie below N/2)
+    const size_t jdk = (size_t)(my < 0 ? my + ndk : my);
     const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT || epi == SPEC_DOT_ABS;
     const bool use_dk = epi == SPEC_DOT || epi == SPEC_DOT_ABS;
     V a[G::R];
@@ -559,7 +566,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
                 }
             }
             bits[e] = b;
-            dv[e] = (b && use_dk) ? dk[((size_t)i * N + j) * dk_stride + h] : czero<V>();
+            dv[e] = (b && use_dk) ? dk[((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h] : czero<V>();
         }
     }
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
@@ -609,7 +616,8 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     double acc[MAX_DOT_SHELLS];
 #pragma unroll
     for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = 0.0;
-    const double wgt = (double)(herm_weight(h, N) * (quad && j != 0 && j != N / 2 ? 2 : 1));
+    // DOT sums carry `weight` (the (N_field / N)^3 of a sub-grid product spectrum)
+    const double wgt = (double)(herm_weight(h, N) * (quad && j != 0 && j != N / 2 ? 2 : 1)) * (use_dk ? weight : 1.0);
     const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
 #pragma unroll
     for (int e = 0; e < G::R; e++) {

@@ -71,13 +71,15 @@ template <typename T, int N> struct L3 {
         stockham_table<V, N / 2, RG::R>(twr);
     }
     // quad: the xy-quadrant layout of data even in x and y ([i <= N/2][j <= N/2][h])
+    // nsrc: grid size of the source spectrum src (0: N; a larger field grid
+    // when this N-grid holds a band-limited sub-grid transform)
     static int inv_x(cudaStream_t st, const V* src, int ss, V* dst, int ds, int mode, const Shell* sh,
-                     int hvalid, const Tables<T>& tb, int quad = 0)
+                     int hvalid, const Tables<T>& tb, int quad = 0, int nsrc = 0)
     {
         PS_LTRY(set_smem(k_inv_x<T, N>, PG::SMEM));
         const int nj = quad ? N / 2 + 1 : N;
         k_inv_x<T, N><<<(unsigned)(nj * (ds / PG::W)), PG::THREADS, PG::SMEM, st>>>(
-            src, ss, dst, ds, mode, sh, hvalid, quad, tb.twp);
+            src, ss, nsrc > 0 ? nsrc : N, dst, ds, mode, sh, hvalid, quad, tb.twp);
         return PS_OK;
     }
     static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb, int quad = 0)
@@ -126,17 +128,18 @@ template <typename T, int N> struct L3 {
                                                         tb.twpp);
         return PS_OK;
     }
+    // ndk: grid size of the field spectrum dk (0: N)
     static int fwd_x(cudaStream_t st, V* data, int stride, int hvalid, int epi, V* out, int ostride,
                      const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
                      int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0,
-                     int quad = 0)
+                     int quad = 0, int ndk = 0)
     {
         PS_LTRY(set_smem(k_fwd_x<T, N>, PG::SMEM));
         const int nj = quad ? N / 2 + 1 : N;
         const unsigned blocks = (unsigned)(nj * (stride / PG::W));
         k_fwd_x<T, N><<<blocks, PG::THREADS, PG::SMEM, st>>>(
-            data, stride, hvalid, epi, out, ostride, dk, dks, shells, nshell, lut, lut_size, weight, quad, partials,
-            tb.twp);
+            data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
+            weight, quad, partials, tb.twp);
         if (nblocks) *nblocks = (int)blocks;
         return PS_OK;
     }

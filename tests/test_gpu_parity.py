@@ -270,3 +270,20 @@ def test_plan_outliving_context(gpu_lib):
     assert ctx.launch_count() > n0
     ctx.close()
     plan.close()
+
+
+@pytest.mark.parametrize("kb", [0, 1, 2, 3])
+@pytest.mark.parametrize("n_grid", [64, 128])
+def test_subgrid_groups_match_oracle(gpu_lib, ora, n_grid, kb):
+    """Theta sweeps whose legs and closing shells are small against the grid run
+    their pair group on a smaller alias-free grid (16 or 32 points for these
+    shells); results match the oracle's N-grid sums, counts exactly."""
+    box = 200.0
+    kf = 2 * np.pi / box
+    case = dict(n=3, equilateral=0, k1=2.2 * kf, k2=3.6 * kf, num_values=7, theta=0.0, kbinwidth=1.0,
+                kbinning=kb, dcos_theta=0.2, use_only_phase=1, which_field=2)
+    ref, got = run_both(gpu_lib, ora, n_grid, box, case, 2)
+    check(ref, got, 2, f"N={n_grid} kb={kb}")
+    if kb == 1:
+        np.testing.assert_array_equal(got.kmin, ref.kmin)
+        np.testing.assert_array_equal(got.kmax, ref.kmax)
