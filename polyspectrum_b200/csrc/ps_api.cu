@@ -61,7 +61,10 @@ int fail(int code, const char* fmt, ...)
     case 32: { constexpr int NN = 32; BODY; } break;   \
     case 64: { constexpr int NN = 64; BODY; } break;   \
     case 128: { constexpr int NN = 128; BODY; } break; \
+    case 192: { constexpr int NN = 192; BODY; } break; \
     case 256: { constexpr int NN = 256; BODY; } break; \
+    case 320: { constexpr int NN = 320; BODY; } break; \
+    case 384: { constexpr int NN = 384; BODY; } break; \
     case 512: { constexpr int NN = 512; BODY; } break; \
     case 1024: { constexpr int NN = 1024; BODY; } break; \
     default: return fail(PS_ERR_UNSUPPORTED, "grid size %d not supported", N); \
@@ -155,7 +158,10 @@ template <typename T> int pw(int N)
     case 32: return PencilGeom<T, 32>::W;
     case 64: return PencilGeom<T, 64>::W;
     case 128: return PencilGeom<T, 128>::W;
+    case 192: return PencilGeom<T, 192>::W;
     case 256: return PencilGeom<T, 256>::W;
+    case 320: return PencilGeom<T, 320>::W;
+    case 384: return PencilGeom<T, 384>::W;
     case 512: return PencilGeom<T, 512>::W;
     default: return PencilGeom<T, 1024>::W;
     }
@@ -1013,7 +1019,7 @@ struct LegKey {
     }
 };
 
-// Smallest transform size M (a power of two, 16 <= M <= N) on which a pair
+// Smallest transform size M (16 <= M <= N, one of the instantiated sizes) on which a pair
 // group with leg bands ba, bb (largest |component| of a mode) and closing
 // bands up to bc runs alias-free.  A triple m_a + m_b + m_c = 0 (mod M) with
 // each component of |m_i| <= b_i and b_a + b_b + b_c < M is zero outright, so
@@ -1022,9 +1028,10 @@ struct LegKey {
 // keeps every mode of a shell on its own M-grid index.  N when none fits.
 int alias_free_grid(int N, int ba, int bb, int bc)
 {
+    static const int sizes[] = {16, 32, 64, 128, 192, 256, 320, 384, 512, 1024};
     const int bmax = std::max({ba, bb, bc});
-    for (int M = 16; M < N; M *= 2)
-        if (M > ba + bb + bc && M > 2 * bmax) return M;
+    for (int M : sizes)
+        if (M < N && M > ba + bb + bc && M > 2 * bmax) return M;
     return N;
 }
 

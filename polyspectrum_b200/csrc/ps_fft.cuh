@@ -2,8 +2,9 @@
 //
 // A transform of length N is done by TPF = N/R threads.  Thread t holds
 // a[e] = x[t + TPF*e] ("canonical layout") on entry and X[t + TPF*e] on exit.
-// Passes are radix-R (the last one may be a smaller radix, each thread then
-// does R/Rp butterflies).  Pass p with radix Rp and span Ns (product of the
+// N is a power of two, or 3 or 5 times one (sub-grid transforms).  Passes are
+// radix-R (for N = f 2^k, R = f 2^r: one radix-R pass, then radix 2^r), the
+// last one possibly of a smaller radix; each thread then does R/Rp butterflies.  Pass p with radix Rp and span Ns (product of the
 // previous radices) computes, for butterfly v in [0, N/Rp):
 //     b_q = x[v + q*N/Rp] * W_{Ns*Rp}^{q*(v mod Ns)},  b = DFT_Rp(b),
 //     y[(v/Ns)*Ns*Rp + (v mod Ns) + q*Ns] = b_q
@@ -35,6 +36,40 @@ __device__ __forceinline__ constexpr double cos32(int j)
     return cos32(32 - j);
 }
 
+// cos(2 pi p / q) for integers p, q > 0, evaluated at compile time: the angle
+// is folded into [0, pi/4] by the exact symmetries of cos and sin on the
+// rational p/q, then summed as a Taylor series (13 terms; the remainder is
+// below 1e-24 there).  For the radix-3 / radix-5 constants, whose angles are
+// not multiples of pi/16.
+__host__ __device__ constexpr double taylor_cos(double t)
+{
+    double term = 1.0, sum = 1.0;
+    for (int i = 1; i <= 13; i++) {
+        term *= -t * t / ((2.0 * i - 1.0) * (2.0 * i));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double taylor_sin(double t)
+{
+    double term = t, sum = t;
+    for (int i = 1; i <= 13; i++) {
+        term *= -t * t / ((2.0 * i) * (2.0 * i + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double cos_2pi(long long p, long long q)
+{
+    p %= q;
+    if (p < 0) p += q;
+    if (2 * p > q) p = q - p;                                  // cos(2pi(1-x)) = cos(2pi x)
+    if (4 * p > q) return -cos_2pi(q - 2 * p, 2 * q);          // x > 1/4: -cos(2pi(1/2-x))
+    if (8 * p > q) return taylor_sin(6.283185307179586477 * (double)(q - 4 * p) / (double)(4 * q));
+    return taylor_cos(6.283185307179586477 * (double)p / (double)q);
+}
+__host__ __device__ constexpr double sin_2pi(long long p, long long q) { return cos_2pi(q - 4 * p, 4 * q); }
+
 // W_R^k for the forward (e^{-}) or inverse (e^{+}) direction, applied to v.
 template <int R, int K, bool INV, typename V> __device__ __forceinline__ V twiddle_const(V v)
 {
@@ -42,6 +77,12 @@ template <int R, int K, bool INV, typename V> __device__ __forceinline__ V twidd
         return v;
     } else if constexpr (4 * K == R) {
         return mul_mi<INV>(v);
+    } else if constexpr (32 % R != 0) {
+        using T = decltype(v.x);
+        constexpr double cd = cos_2pi(K, R), sd = sin_2pi(K, R);
+        const T c = (T)cd;
+        const T s = INV ? (T)sd : (T)-sd;
+        return V{v.x * c - v.y * s, v.x * s + v.y * c};
     } else {
         using T = decltype(v.x);
         constexpr int j = K * (32 / R);
@@ -51,8 +92,10 @@ template <int R, int K, bool INV, typename V> __device__ __forceinline__ V twidd
     }
 }
 
-// Decimation-in-frequency DFT of length R in registers, natural order in and out.
+// Decimation-in-frequency DFT of length R in registers, natural order in and
+// out: even R splits into two halves, R = 3 and 5 are direct butterflies.
 template <int R, bool INV> struct Dft {
+    static_assert(R % 2 == 0, "odd DFT lengths other than 3 and 5 are not provided");
     template <typename V> static __device__ __forceinline__ void run(V* a)
     {
         constexpr int H = R / 2;
@@ -78,15 +121,65 @@ template <int R, bool INV> struct Dft {
 template <bool INV> struct Dft<1, INV> {
     template <typename V> static __device__ __forceinline__ void run(V*) {}
 };
+// y_k = sum_n a_n W_3^{nk}: y0 = a0 + s, y1,2 = a0 - s/2 -/+ i sin(2pi/3) d
+// (forward), s = a1 + a2, d = a1 - a2; the inverse swaps the +/- i terms.
+template <bool INV> struct Dft<3, INV> {
+    template <typename V> static __device__ __forceinline__ void run(V* a)
+    {
+        using T = decltype(a[0].x);
+        constexpr T s3 = (T)sin_2pi(1, 3);
+        const V s = cadd(a[1], a[2]), d = csub(a[1], a[2]);
+        const V t = V{a[0].x - (T)0.5 * s.x, a[0].y - (T)0.5 * s.y};
+        const V u = V{-s3 * d.y, s3 * d.x};  // i sin(2pi/3) d
+        a[0] = cadd(a[0], s);
+        a[1] = INV ? cadd(t, u) : csub(t, u);
+        a[2] = INV ? csub(t, u) : cadd(t, u);
+    }
+};
+// Length 5: with t1 = a1 + a4, t2 = a2 + a3, d1 = a1 - a4, d2 = a2 - a3,
+// y0 = a0 + t1 + t2, y1,4 = a0 + c1 t1 + c2 t2 -/+ i (s1 d1 + s2 d2),
+// y2,3 = a0 + c2 t1 + c1 t2 -/+ i (s2 d1 - s1 d2) (forward signs),
+// c_j = cos(2pi j/5), s_j = sin(2pi j/5).
+template <bool INV> struct Dft<5, INV> {
+    template <typename V> static __device__ __forceinline__ void run(V* a)
+    {
+        using T = decltype(a[0].x);
+        constexpr T c1 = (T)cos_2pi(1, 5), c2 = (T)cos_2pi(2, 5);
+        constexpr T s1 = (T)sin_2pi(1, 5), s2 = (T)sin_2pi(2, 5);
+        const V t1 = cadd(a[1], a[4]), t2 = cadd(a[2], a[3]);
+        const V d1 = csub(a[1], a[4]), d2 = csub(a[2], a[3]);
+        const V r1 = V{a[0].x + c1 * t1.x + c2 * t2.x, a[0].y + c1 * t1.y + c2 * t2.y};
+        const V r2 = V{a[0].x + c2 * t1.x + c1 * t2.x, a[0].y + c2 * t1.y + c1 * t2.y};
+        const V p1 = V{s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y};
+        const V p2 = V{s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y};
+        const V i1 = V{-p1.y, p1.x}, i2 = V{-p2.y, p2.x};  // i p
+        a[0] = cadd(a[0], cadd(t1, t2));
+        a[1] = INV ? cadd(r1, i1) : csub(r1, i1);
+        a[4] = INV ? csub(r1, i1) : cadd(r1, i1);
+        a[2] = INV ? cadd(r2, i2) : csub(r2, i2);
+        a[3] = INV ? csub(r2, i2) : cadd(r2, i2);
+    }
+};
 
-// Radix plan: passes of radix R while possible, then one pass of the remainder.
+// Radix plan.  R = f 2^r with f in {1, 3, 5} the odd part of N: for f = 1,
+// passes of radix R while possible, then one pass of the remainder; for f > 1
+// one pass of radix R first (it carries the odd factor), then the same scheme
+// with radix 2^r on N / R.  Every radix divides R.
 template <int N, int R> struct RadixPlan {
-    __host__ __device__ static constexpr int count_full(int n) { return n >= R ? 1 + count_full(n / R) : 0; }
-    __host__ __device__ static constexpr int rem_of(int n) { return n >= R ? rem_of(n / R) : n; }
-    static constexpr int FULL = count_full(N);
-    static constexpr int REM = rem_of(N);  // 1 if N is a power of R
-    static constexpr int P = FULL + (REM > 1 ? 1 : 0);
-    __host__ __device__ static constexpr int radix(int p) { return p < FULL ? R : REM; }
+    __host__ __device__ static constexpr int odd_of(int n) { return n % 2 ? n : odd_of(n / 2); }
+    static constexpr int F = odd_of(R);
+    static constexpr int R2 = R / F;                  // radix of the power-of-two passes
+    static constexpr int HEAD = F > 1 ? 1 : 0;        // the radix-R pass of a mixed length
+    static constexpr int N2 = N / (F > 1 ? R : 1);    // what the power-of-two passes cover
+    __host__ __device__ static constexpr int count_full(int n) { return n >= R2 ? 1 + count_full(n / R2) : 0; }
+    __host__ __device__ static constexpr int rem_of(int n) { return n >= R2 ? rem_of(n / R2) : n; }
+    static constexpr int FULL = count_full(N2);
+    static constexpr int REM = rem_of(N2);  // 1 if N2 is a power of R2
+    static constexpr int P = HEAD + FULL + (REM > 1 ? 1 : 0);
+    __host__ __device__ static constexpr int radix(int p)
+    {
+        return p < HEAD ? R : (p < HEAD + FULL ? R2 : REM);
+    }
     __host__ __device__ static constexpr int span(int p)
     {
         int s = 1;
@@ -101,13 +194,17 @@ template <int N, int R> struct RadixPlan {
         for (int q = 0; q < p; q++) o += span(q) * (radix(q) - 1);
         return o;
     }
-    static_assert(R >= 2 && (R & (R - 1)) == 0, "radix must be a power of two");
-    static_assert((N & (N - 1)) == 0 && N >= R, "length must be a power of two >= R");
+    static_assert(F == 1 || F == 3 || F == 5, "radix must be 2^r, 3*2^r or 5*2^r");
+    static_assert(R2 >= 2 || F > 1, "power-of-two radix must be >= 2");
+    static_assert(N % R == 0 && odd_of(N) == F, "length must be R times a power of two");
+    static_assert(F == 1 || R2 >= 2 || N == R, "mixed lengths need a power-of-two part in R");
 };
 
-// Elements per thread used for each transform length.
+// Elements per thread used for each transform length (3 2^k and 5 2^k: the
+// odd factor times 4, 16 or 32 threads per transform).
 template <int N> struct DefaultRadix {
-    static constexpr int value = N <= 16 ? N : (N == 32 || N == 64 || N == 128 || N == 512) ? 8 : 16;
+    static constexpr int value = N == 96 ? 12 : N == 160 ? 20 : N == 192 ? 12 : N == 320 ? 20 : N == 384 ? 12
+                               : N <= 16 ? N : (N == 32 || N == 64 || N == 128 || N == 512) ? 8 : 16;
 };
 
 // Synchronisation between passes: the whole CTA (pencil kernels, whose
@@ -147,7 +244,7 @@ __device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* _
 #pragma unroll
             for (int q = 0; q < Rp; q++) b[q] = a[u + q * BPT];
             const int v = t + TPF * u;
-            const int k = v & (Ns - 1);
+            const int k = v % Ns;
             if constexpr (Ns > 1) {
                 const V* tp = twt + Plan::tw_off(P_) + k * (Rp - 1);
 #pragma unroll

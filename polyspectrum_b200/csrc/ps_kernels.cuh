@@ -54,15 +54,24 @@ template <typename T, int N> struct PencilGeom {
 // at most 32 threads per row (warp-synchronous) except FP64 rows of 512,
 // which use radix 8 and 64 threads (two transforms must fit in registers).
 template <typename T, int NH> struct RowRadix {
-    static constexpr int value = NH <= 16 ? NH : ((sizeof(T) == 4 && NH == 512) ? 16 : 8);
+    static constexpr bool POW2 = (NH & (NH - 1)) == 0;
+    static constexpr int value = !POW2 ? DefaultRadix<NH>::value
+                               : NH <= 16 ? NH : ((sizeof(T) == 4 && NH == 512) ? 16 : 8);
 };
 template <typename T, int N> struct RowGeom {
     static constexpr int NH = N / 2;
     static constexpr int R = RowRadix<T, NH>::value;
     static constexpr int TPF = NH / R;
-    static constexpr int WZ = (256 / TPF) < 32 ? (256 / TPF) : 32;  // rows per CTA (tile)
-    static constexpr int THREADS = TPF * WZ;
     static constexpr int EPC = 16 / (int)sizeof(V2<T>);  // complex elements per 16-byte copy
+    // rows per CTA (tile): up to 256 threads and 32 rows, and as many as fit
+    // in 227 KB of shared memory with two double-buffered full-length inputs
+    static constexpr int WZ0 = (256 / TPF) < 32 ? (256 / TPF) : 32;
+    static constexpr size_t ROW_BYTES =
+        (size_t)(NH + 4 * ((NH + 1 + EPC - 1) / EPC * EPC)) * sizeof(V2<T>);
+    static constexpr int WZ_FIT = (int)((227 * 1024 - (size_t)(2 * NH + 2) * sizeof(V2<T>)) / ROW_BYTES);
+    __host__ __device__ static constexpr int pow2_floor(int v) { return v >= 2 ? 2 * pow2_floor(v / 2) : 1; }
+    static constexpr int WZ = pow2_floor(WZ0 < WZ_FIT ? WZ0 : WZ_FIT);
+    static constexpr int THREADS = TPF * WZ;
     // shared memory: row Stockham table [NH], pre/post twiddles W_N^k, k <= NH
     // [NH+2], per-row exchange buffers [WZ][NH], then the input stages
     static constexpr size_t TWR_OFF = 0;
@@ -77,6 +86,8 @@ template <typename T, int N> struct RowGeom {
         return STAGE_OFF + (size_t)2 * WZ * (pitch(hva) + (ninputs > 1 ? pitch(hvb) : 0)) * sizeof(V2<T>);
     }
     static_assert(TPF <= 32 || WZ <= 15, "one named barrier per row");
+    static_assert(THREADS % 32 == 0, "whole warps per CTA");
+    static_assert(smem(2, NH + 1, NH + 1) <= 227 * 1024, "row tile exceeds shared memory");
 };
 
 // Copy a twiddle table into shared memory (whole CTA).
@@ -298,8 +309,8 @@ __device__ __forceinline__ void r2c_row(V2<T> (&a)[RowGeom<T, N>::R], RowCtx<T, 
     rc.sync();
     const T half = (T)0.5;
     for (int k = rc.t; k <= NH && k < hout; k += G::TPF) {
-        const V yk = sm.ld(k & (NH - 1));
-        const V ym = cconj(sm.ld((NH - k) & (NH - 1)));
+        const V yk = sm.ld(k == NH ? 0 : k);
+        const V ym = cconj(sm.ld(k == 0 ? 0 : NH - k));
         const V E = V{(yk.x + ym.x) * half, (yk.y + ym.y) * half};
         const V D = csub(yk, ym);
         const V O = V{D.y * half, -D.x * half};  // D / (2i)

@@ -145,12 +145,17 @@ template <typename T, int N> struct L3 {
     }
 };
 
+// Grid sizes: the powers of two a context runs on, and 3 2^k / 5 2^k sizes
+// for the alias-free sub-grids of pair groups.
 #define PS_INSTANTIATE_L3(T)          \
     template struct L3<T, 16>;        \
     template struct L3<T, 32>;        \
     template struct L3<T, 64>;        \
     template struct L3<T, 128>;       \
+    template struct L3<T, 192>;       \
     template struct L3<T, 256>;       \
+    template struct L3<T, 320>;       \
+    template struct L3<T, 384>;       \
     template struct L3<T, 512>;       \
     template struct L3<T, 1024>;
 
@@ -159,7 +164,10 @@ template <typename T, int N> struct L3 {
     extern template struct L3<T, 32>;    \
     extern template struct L3<T, 64>;    \
     extern template struct L3<T, 128>;   \
+    extern template struct L3<T, 192>;   \
     extern template struct L3<T, 256>;   \
+    extern template struct L3<T, 320>;   \
+    extern template struct L3<T, 384>;   \
     extern template struct L3<T, 512>;   \
     extern template struct L3<T, 1024>;
 

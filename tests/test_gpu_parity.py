@@ -287,3 +287,32 @@ def test_subgrid_groups_match_oracle(gpu_lib, ora, n_grid, kb):
     if kb == 1:
         np.testing.assert_array_equal(got.kmin, ref.kmin)
         np.testing.assert_array_equal(got.kmax, ref.kmax)
+
+
+@pytest.mark.parametrize("n_grid,pairs", [(256, [(0.5, 0.8)]), (512, [(0.8, 1.2), (1.0, 1.5)])],
+                         ids=["N256_subgrid192", "N512_subgrid320_384"])
+def test_mixed_radix_subgrids_match_plain(gpu_lib, n_grid, pairs):
+    """DERIVED theta sweeps of the bench workload whose pair groups run on
+    192-, 320- and 384-point sub-grids (radix-3 and radix-5 transforms): the
+    batched FP32 method against the plain FP64 method (the reference dataflow
+    on the full grid) on the same XHI_DENS phase field, B within the batched
+    tolerance, counts and derived ranges identical."""
+    from polyspectrum_b200 import synth
+    ps = gpu_lib
+    box = 400.0
+    dens, xhii = synth.xhi_dens_inputs(n_grid, box, int(round(32000 * (n_grid / 512) ** 3)), 3, 2.0, 4)
+    cfgs = []
+    for k1, k2 in pairs:
+        c, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1, k2=k2, num_values=16,
+                                             kbinningCase=ps.PS_BIN_DERIVED)
+        cfgs += [c[i] for i in range(len(c))]
+    with ps.Context(n_grid, box) as ctx:
+        ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+        B32, N32, _, out32 = ctx.batch(cfgs, ps.PS_FP32_BATCHED)
+        B64, N64, _, out64 = ctx.batch(cfgs, ps.PS_FP64_PLAIN)
+    scale = np.abs(B64).max()
+    assert np.all(np.abs(B32 - B64) <= 1e-5 * np.abs(B64) + 1e-6 * scale), (B32, B64)
+    np.testing.assert_array_equal(N32, np.rint(N64))
+    for i in range(len(cfgs)):
+        assert list(out32[i].kmin)[:3] == list(out64[i].kmin)[:3]
+        assert list(out32[i].kmax)[:3] == list(out64[i].kmax)[:3]
