@@ -575,9 +575,13 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
         PS_TRY(ensure_partials(c, blocks * MAX_DOT_SHELLS));
         bool lut_ok = true;
         int lut_size = 0;
+        long long r2max = 0;  // no mode of these shells lies outside |m|^2 <= r2max
         for (int q = s0; q < s0 + cnt; q++) {
             if (hsh[q].kind != SHELL_DEFAULT && hsh[q].kind != SHELL_RANGE) lut_ok = false;
             lut_size = std::max(lut_size, hsh[q].r2hi + 1);
+            const long long b = std::min(hsh[q].band, N / 2);
+            r2max = std::max(r2max, (hsh[q].kind == SHELL_DEFAULT || hsh[q].kind == SHELL_RANGE)
+                                        ? (long long)hsh[q].r2hi : 3 * b * b);
         }
         const unsigned short* lut = nullptr;
         if (lut_ok) {
@@ -593,7 +597,7 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
             Prof pf(c);
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, data, S, hvalid, epi, nullptr, 0, B.spec, B.S,
                                                     dshells + s0, cnt, lut, lut_size, c->partials, tb, &nb,
-                                                    weight, quad, c->N))));
+                                                    weight, quad, c->N, (int)std::min<long long>(r2max, 0x7fffffff)))));
             const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / ((double)N * N) : 1.0;
             pf.end(fam<T>(KF_FWD_X_DOT), q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
         }
@@ -648,6 +652,16 @@ Shell make_shell(int kind, double k, double kmin, double kmax, double binwidth, 
     return s;
 }
 
+// Grid of k_derived_range: one thread per (mx, my) column for interval shells,
+// per mode of the band cube otherwise.
+int derived_blocks(const Shell& sh, int band)
+{
+    const long long side = 2 * band + 1;
+    const long long total = (sh.kind == SHELL_DEFAULT || sh.kind == SHELL_RANGE) ? side * side
+                                                                                : side * side * (band + 1);
+    return (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 16));
+}
+
 // DERIVED ranges (filter.c:78-114) of DEFAULT shells, computed on the device.
 int derive_ranges(ps_gpu_ctx* c, const std::vector<Shell>& sh, std::vector<double>& kmin,
                   std::vector<double>& kmax)
@@ -670,8 +684,7 @@ int derive_ranges(ps_gpu_ctx* c, const std::vector<Shell>& sh, std::vector<doubl
     for (int s = 0; s < ns; s++) {
         const int band = std::min(sh[s].band, N / 2);
         const int hmax = band;
-        const long long total = (long long)(2 * band + 1) * (2 * band + 1) * (hmax + 1);
-        const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+        const int blocks = derived_blocks(sh[s], band);
         Prof pf(c);
         k_derived_range<<<blocks, 256, 0, c->stream>>>(N, c->dshells + s, hmax, c->dminmax + 2 * s);
         pf.end(KF_DERIVED, 0.0);
@@ -1306,8 +1319,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             PS_CK(cudaMemcpyAsync(dmm, dmm_init, 16 * (size_t)nd, cudaMemcpyDeviceToDevice, c->stream));
             for (int q = 0; q < nd; q++) {
                 const int band = std::min(derived[q].band, N / 2);
-                const long long total = (long long)(2 * band + 1) * (2 * band + 1) * (band + 1);
-                const int blocks = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 16));
+                const int blocks = derived_blocks(derived[q], band);
                 Prof pf(c);
                 k_derived_range<<<blocks, 256, 0, c->stream>>>(N, dderived + q, band, dmm + 2 * q);
                 pf.end(KF_DERIVED, 0.0);

@@ -527,12 +527,17 @@ enum SpecEpi : int {
     SPEC_DOT_ABS = 5       // as SPEC_DOT with |term| (condition numbers)
 };
 
-template <typename T, int N>
-__global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
+// DOT: true for the per-shell sum epilogues (SPEC_DOT, SPEC_COUNT,
+// SPEC_DOT_ABS), false for the storing ones; the two are separate
+// instantiations so the storing pass is not sized for the sums' registers.
+// r2max (sums only): no shell of the launch holds a mode with |m|^2 > r2max,
+// so a tile of pencils whose (my, mz) lie outside that ball is skipped.
+template <typename T, int N, bool DOT>
+__global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) == 8) ? 1 : 2)
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, int ndk, const Shell* __restrict__ shells,
             int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight, int quad,
-            double* __restrict__ partials, const V2<T>* __restrict__ tw_g)
+            int r2max, double* __restrict__ partials, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
@@ -547,26 +552,29 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     const bool col_ok = h < hvalid && h <= N / 2;
     const int my = lattice_freq(j, N);
     const int mz = h == N / 2 ? -(N / 2) : h;
-    // dk: field spectrum of an ndk-grid ([ndk][ndk][dk_stride], ndk >= N); mode m
-    // of this grid sits at index m mod ndk there (the shells lie below N/2)
-    const size_t jdk = (size_t)(my < 0 ? my + ndk : my);
-    const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT || epi == SPEC_DOT_ABS;
-    const bool use_dk = epi == SPEC_DOT || epi == SPEC_DOT_ABS;
+    if constexpr (DOT) {
+        // the whole tile outside every shell: no transform, zero partials
+        const bool live = col_ok && my * my + mz * mz <= r2max;
+        if (!__syncthreads_or(live)) {
+            if (threadIdx.x < nshell) partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = 0.0;
+            return;
+        }
+    }
     V a[G::R];
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int i = t + G::TPF * e;
         a[e] = data[((size_t)(quad && i > N / 2 ? N - i : i) * nj + j) * stride + h];
     }
-    // dot / count: the shell bits depend on indices only, so they and the
-    // field values they need are fetched before the transform
-    unsigned bits[G::R];
-    V dv[G::R];
-    if (dot) {
+    // sums: the shell bits depend on indices only and are found before the
+    // transform (16 bits per mode, two modes per register)
+    unsigned bits2[(G::R + 1) / 2];
+    if constexpr (DOT) {
+#pragma unroll
+        for (int e = 0; e < (G::R + 1) / 2; e++) bits2[e] = 0u;
 #pragma unroll
         for (int e = 0; e < G::R; e++) {
-            const int i = t + G::TPF * e;
-            const int mx = lattice_freq(i, N);
+            const int mx = lattice_freq(t + G::TPF * e, N);
             unsigned b = 0u;
             if (col_ok) {
                 if (lut) {
@@ -576,15 +584,14 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
                     b = shell_bits(shells, nshell, mx, my, mz);
                 }
             }
-            bits[e] = b;
-            dv[e] = (b && use_dk) ? dk[((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h] : czero<V>();
+            bits2[e / 2] |= (b & 0xffffu) << (16 * (e & 1));
         }
     }
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
     __syncthreads();
     SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), w};
     fft_passes<V, N, G::R, false>(a, t, sm, tw, BlockSync{});
-    if (!dot) {
+    if constexpr (!DOT) {
         unsigned keep = (1u << G::R) - 1u;
         if (epi == SPEC_MASK_ADD) {
             keep = 0u;
@@ -619,44 +626,56 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
             }
             out[((size_t)i * N + j) * out_stride + h] = v;
         }
-        return;
-    }
-    // per-shell FP64 sums in registers, then one fixed-order reduction for all
-    // shells at once (deterministic): warp xor-trees, per-warp rows in shared
-    // memory, one thread per shell sums the rows in warp order.
-    double acc[MAX_DOT_SHELLS];
+    } else {
+        // dk: field spectrum of an ndk-grid ([ndk][ndk][dk_stride], ndk >= N);
+        // mode m of this grid sits at index m mod ndk there (shells lie below N/2).
+        // Per-shell FP64 sums in registers, then one fixed-order reduction for
+        // all shells at once (deterministic): warp xor-trees, per-warp rows in
+        // shared memory, one thread per shell sums the rows in warp order.
+        const bool use_dk = epi == SPEC_DOT || epi == SPEC_DOT_ABS;
+        const size_t jdk = (size_t)(my < 0 ? my + ndk : my);
+        double acc[MAX_DOT_SHELLS];
 #pragma unroll
-    for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = 0.0;
-    // DOT sums carry `weight` (the (N_field / N)^3 of a sub-grid product spectrum)
-    const double wgt = (double)(herm_weight(h, N) * (quad && j != 0 && j != N / 2 ? 2 : 1)) * (use_dk ? weight : 1.0);
-    const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
+        for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = 0.0;
+        // DOT sums carry `weight` (the (N_field / N)^3 of a sub-grid product spectrum)
+        const double wgt =
+            (double)(herm_weight(h, N) * (quad && j != 0 && j != N / 2 ? 2 : 1)) * (use_dk ? weight : 1.0);
+        const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
 #pragma unroll
-    for (int e = 0; e < G::R; e++) {
-        if (bits[e]) {
-            double val = use_dk ? wgt * ((double)dv[e].x * (double)a[e].x + (double)dv[e].y * (double)a[e].y)
-                                : wgt * rint((double)a[e].x * inv_n3);
-            if (epi == SPEC_DOT_ABS) val = fabs(val);
+        for (int e = 0; e < G::R; e++) {
+            const unsigned b = (bits2[e / 2] >> (16 * (e & 1))) & 0xffffu;
+            if (b) {
+                double val;
+                if (use_dk) {
+                    const int mx = lattice_freq(t + G::TPF * e, N);
+                    const V d = dk[((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h];
+                    val = wgt * ((double)d.x * (double)a[e].x + (double)d.y * (double)a[e].y);
+                } else {
+                    val = wgt * rint((double)a[e].x * inv_n3);
+                }
+                if (epi == SPEC_DOT_ABS) val = fabs(val);
 #pragma unroll
-            for (int c = 0; c < MAX_DOT_SHELLS; c++)
-                if ((bits[e] >> c) & 1u) acc[c] += val;
+                for (int c = 0; c < MAX_DOT_SHELLS; c++)
+                    if ((b >> c) & 1u) acc[c] += val;
+            }
         }
-    }
-    constexpr int NW = G::THREADS / 32;
-    __shared__ double wsum[NW][MAX_DOT_SHELLS];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        constexpr int NW = G::THREADS / 32;
+        __shared__ double wsum[NW][MAX_DOT_SHELLS];
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-    for (int c = 0; c < MAX_DOT_SHELLS; c++) {
-        double v = acc[c];
+        for (int c = 0; c < MAX_DOT_SHELLS; c++) {
+            double v = acc[c];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == c) wsum[wid][c] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < nshell) {
-        double sum = 0.0;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == c) wsum[wid][c] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < nshell) {
+            double sum = 0.0;
 #pragma unroll 1
-        for (int q = 0; q < NW; q++) sum += wsum[q][threadIdx.x];
-        partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = sum;
+            for (int q = 0; q < NW; q++) sum += wsum[q][threadIdx.x];
+            partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = sum;
+        }
     }
 }
 
@@ -806,6 +825,14 @@ static __global__ void k_sum_partials(const double* __restrict__ partials, int n
 // binary64 sqrt(fl(s*s)) = s, so that equals sqrt of the global min/max of the
 // squared corners whatever the visiting order.  Non-negative doubles order
 // like their bit patterns, so the fold is an integer atomicMin/atomicMax.
+__device__ __forceinline__ int isqrt_floor(int v)  // floor(sqrt(v)), v >= 0
+{
+    int r = (int)sqrt((double)v);
+    while (r * r > v) r--;
+    while ((r + 1) * (r + 1) <= v) r++;
+    return r;
+}
+
 static __global__ void k_derived_range(int n, const Shell* __restrict__ shell_p, int hmax,
                                        unsigned long long* minmax_bits)
 {
@@ -813,15 +840,35 @@ static __global__ void k_derived_range(int n, const Shell* __restrict__ shell_p,
     const int band = min(sh.band, n / 2);
     const int side = 2 * band + 1;
     double min2 = sh.min2_init, max2 = 0.0;
-    const long long total = (long long)side * side * (hmax + 1);
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
-        const int hz = (int)(q % (hmax + 1));
-        const long long r = q / (hmax + 1);
-        const int mx = (int)(r / side) - band, my = (int)(r % side) - band;
-        if (mx >= n / 2 || my >= n / 2 || mx < -(n / 2) || my < -(n / 2)) continue;
-        const int mz = hz == n / 2 ? -(n / 2) : hz;
-        if (shell_bit(sh, mx, my, mz)) corners_fold(mx, my, mz, sh.half, min2, max2);
+    if (sh.kind == SHELL_DEFAULT || sh.kind == SHELL_RANGE) {
+        // interval shells: one thread per (mx, my) column, mz over the exact
+        // range r2lo <= mx^2 + my^2 + mz^2 <= r2hi (mz >= 0: the corner radii
+        // of (mx, my, -mz) are those of (mx, my, mz))
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < side * side; q += gridDim.x * blockDim.x) {
+            const int mx = q / side - band, my = q % side - band;
+            if (mx >= n / 2 || my >= n / 2 || mx < -(n / 2) || my < -(n / 2)) continue;
+            const int s = mx * mx + my * my;
+            if (sh.r2hi < 0 || s > sh.r2hi) continue;
+            int z0 = 0;
+            if (sh.r2lo - s > 0) {
+                z0 = isqrt_floor(sh.r2lo - s);
+                if (z0 * z0 < sh.r2lo - s) z0++;
+            }
+            const int z1 = min(isqrt_floor(sh.r2hi - s), hmax);
+            for (int hz = z0; hz <= z1; hz++)
+                corners_fold(mx, my, hz == n / 2 ? -(n / 2) : hz, sh.half, min2, max2);
+        }
+    } else {
+        const long long total = (long long)side * side * (hmax + 1);
+        for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+             q += (long long)gridDim.x * blockDim.x) {
+            const int hz = (int)(q % (hmax + 1));
+            const long long r = q / (hmax + 1);
+            const int mx = (int)(r / side) - band, my = (int)(r % side) - band;
+            if (mx >= n / 2 || my >= n / 2 || mx < -(n / 2) || my < -(n / 2)) continue;
+            const int mz = hz == n / 2 ? -(n / 2) : hz;
+            if (shell_bit(sh, mx, my, mz)) corners_fold(mx, my, mz, sh.half, min2, max2);
+        }
     }
     // min2/max2 are non-negative (or the +huge start value)
     unsigned long long lo = __double_as_longlong(min2), hi = __double_as_longlong(max2);

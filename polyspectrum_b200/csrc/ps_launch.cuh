@@ -128,18 +128,27 @@ template <typename T, int N> struct L3 {
                                                         tb.twpp);
         return PS_OK;
     }
-    // ndk: grid size of the field spectrum dk (0: N)
+    // ndk: grid size of the field spectrum dk (0: N); r2max: bound of the
+    // launch's shells' |m|^2 for the sum epilogues (tiles outside are skipped)
     static int fwd_x(cudaStream_t st, V* data, int stride, int hvalid, int epi, V* out, int ostride,
                      const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
                      int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0,
-                     int quad = 0, int ndk = 0)
+                     int quad = 0, int ndk = 0, int r2max = 0x7fffffff)
     {
-        PS_LTRY(set_smem(k_fwd_x<T, N>, PG::SMEM));
         const int nj = quad ? N / 2 + 1 : N;
         const unsigned blocks = (unsigned)(nj * (stride / PG::W));
-        k_fwd_x<T, N><<<blocks, PG::THREADS, PG::SMEM, st>>>(
-            data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
-            weight, quad, partials, tb.twp);
+        const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT || epi == SPEC_DOT_ABS;
+        if (dot) {
+            PS_LTRY(set_smem(k_fwd_x<T, N, true>, PG::SMEM));
+            k_fwd_x<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(
+                data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
+                weight, quad, r2max, partials, tb.twp);
+        } else {
+            PS_LTRY(set_smem(k_fwd_x<T, N, false>, PG::SMEM));
+            k_fwd_x<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(
+                data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
+                weight, quad, r2max, partials, tb.twp);
+        }
         if (nblocks) *nblocks = (int)blocks;
         return PS_OK;
     }
