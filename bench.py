@@ -212,8 +212,10 @@ def run_ours(args, rank, world, local_rank):
     ctx.set_stream(stream.cuda_stream)
     dens = torch.from_numpy(dens_np).to(dev)
     xhii = torch.from_numpy(xhii_np).to(dev)
-    # the 64 configurations planned once; executions replay one CUDA graph
-    plan = ctx.plan(cfgs, method=ps.PS_FP32_BATCHED, graph=True)
+    # the 64 configurations planned once (transform size of each pair group
+    # autotuned at planning); executions replay one CUDA graph
+    plan = ctx.plan(cfgs, method=ps.PS_FP32_BATCHED, graph=True, autotune=True)
+    tune_table = ctx.tune_export()
 
     def step():
         ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
@@ -278,11 +280,14 @@ def run_ours(args, rank, world, local_rank):
     roof = None
     if dom:
         achieved = dom["bytes"] / (dom["ms"] / 1e3) / 1e9
+        # DRAM bytes per launch of this kernel instance from an ncu capture of the
+        # same workload (profiles/dram_traffic.json), when one was taken
         traffic = None
         try:
             with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
                 tr = json.load(f)
-            traffic = tr.get(dom["name"], {}).get("bytes_per_launch_512")
+            if tr.get("workload") == w["workload"]:
+                traffic = tr["kernels"].get(dom["name"], {}).get("dram_bytes_per_launch")
         except Exception:
             pass
         roof = dict(bound="hbm", kernel=dom["name"], achieved=achieved, peak=peak,
@@ -374,7 +379,8 @@ def run_ours(args, rank, world, local_rank):
                                theta_bins=w["num_values"], configs_per_step=ncfg,
                                binning="DERIVED", kbinwidth=1.0, use_only_phase=1,
                                l2="inputs (2 x 512 MiB) and every pass larger than L2; no flush",
-                               parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+                               parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                               subgrids=[int(ln.split()[-1]) for ln in tune_table.splitlines() if ln.startswith("grid")]),
                    e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d,
                             d2h_bytes_per_step=d2h, ms_per_step=ms_e2e / args.steps,
                             mode="pipelined: ps_gpu_set_field_async + ps_gpu_plan_submit per step, "

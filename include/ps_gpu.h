@@ -142,6 +142,13 @@ int ps_gpu_polyspectrum_batch(ps_gpu_ctx *ctx, int method, int nconf, ps_cfg *cf
  * one by one (no graph). */
 #define PS_PLAN_GRAPH 1
 #define PS_PLAN_KAPPA 2
+/* PS_PLAN_AUTOTUNE: each pair group (configurations sharing two legs) runs its
+ * transforms on an alias-free sub-grid; by default the smallest one, with this
+ * flag the fastest of the smallest and up to two larger supported sizes, timed
+ * at plan creation.  Counts are identical either way; sums differ only by FP32
+ * rounding.  Choices are kept per context and can be exported / imported
+ * (ps_gpu_tune_export / ps_gpu_tune_import) so later runs use the same sizes. */
+#define PS_PLAN_AUTOTUNE 4
 typedef struct ps_gpu_plan ps_gpu_plan;
 int ps_gpu_plan_create(ps_gpu_ctx *ctx, int method, int nconf, const ps_cfg *cfgs, int flags,
                        ps_gpu_plan **plan);
@@ -172,6 +179,14 @@ int ps_gpu_set_field_async(ps_gpu_ctx *ctx, int which, const void *dens, const v
 int ps_gpu_plan_submit(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
                        double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
 int ps_gpu_synchronize(ps_gpu_ctx *ctx);
+
+/* The context's autotuned choices as text, one "grid N b_a b_b b_c M" line per
+ * pair-group signature: writes at most buflen bytes (NUL-terminated) and
+ * returns the length of the whole text, or a negative status.  Import adds
+ * the lines of such a text to the context's choices (unknown or malformed
+ * lines: PS_ERR_ARG, nothing imported).  No reference counterpart. */
+int ps_gpu_tune_export(ps_gpu_ctx *ctx, char *buf, int buflen);
+int ps_gpu_tune_import(ps_gpu_ctx *ctx, const char *text);
 
 /* Kernels the context has executed since its creation (a graph replay counts
  * the kernels in the graph); -1 for a NULL context. */
@@ -206,7 +221,8 @@ int ps_gpu_last_timing(ps_gpu_ctx *ctx, double *ms, long long *kernel_launches);
  * launches is bracketed by CUDA events on the context's stream and charged,
  * with its algorithmic HBM bytes (the bytes its pass must read and write at
  * minimum), to its kernel family (FP64 instances of the transform kernels
- * as "<family>_f64").  ps_gpu_kernel_stats synchronises and
+ * as "<family>_f64"), one entry per transform size ("<family>@<size>").
+ * ps_gpu_kernel_stats synchronises and
  * returns up to max families; the counters reset when profiling is switched
  * on.  No reference counterpart (the reference has only a total wall time,
  * main.c:38-82). */

@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
     L.ps_gpu_synchronize.argtypes = [vp]
     L.ps_gpu_launch_count.argtypes = [vp]
     L.ps_gpu_launch_count.restype = C.c_longlong
+    L.ps_gpu_tune_export.argtypes = [vp, C.c_char_p, ip]
+    L.ps_gpu_tune_import.argtypes = [vp, C.c_char_p]
     L.ps_gpu_set_profiling.argtypes = [vp, ip]
     L.ps_gpu_kernel_stats.argtypes = [vp, C.POINTER(ps_kernel_stat), ip]
     L.ps_gpu_finalize.argtypes = [vp]
@@ -100,7 +102,8 @@ def lib() -> C.CDLL:
                  "ps_gpu_polyspectrum_batch", "ps_gpu_grad", "ps_make_configs",
                  "ps_gpu_set_stream", "ps_gpu_last_timing", "ps_gpu_set_profiling",
                  "ps_gpu_kernel_stats", "ps_gpu_plan_create", "ps_gpu_plan_execute",
-                 "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize"):
+                 "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize",
+                 "ps_gpu_tune_export", "ps_gpu_tune_import"):
         getattr(L, name).restype = ip
     _lib = L
     return L
@@ -259,9 +262,20 @@ class Context:
                                                _dptr(kap) if kappa else None))
         return B, Np, kap, arr
 
-    def plan(self, cfgs, method: int = PS_FP32_BATCHED, graph: bool = True, kappa: bool = False):
+    def plan(self, cfgs, method: int = PS_FP32_BATCHED, graph: bool = True, kappa: bool = False,
+             autotune: bool = False):
         """A reusable plan of these configurations (ps_gpu_plan_create)."""
-        return Plan(self, cfgs, method, graph, kappa)
+        return Plan(self, cfgs, method, graph, kappa, autotune)
+
+    def tune_export(self) -> str:
+        """The autotuned sub-grid choices of this context (ps_gpu_tune_export)."""
+        n = _check(lib().ps_gpu_tune_export(self._h, None, 0))
+        buf = C.create_string_buffer(n + 1)
+        _check(lib().ps_gpu_tune_export(self._h, buf, n + 1))
+        return buf.value.decode()
+
+    def tune_import(self, text: str):
+        _check(lib().ps_gpu_tune_import(self._h, text.encode()))
 
     def grad(self, n, k, kmin, kmax, kbinwidth, kbinningCase, method=PS_FP64_PLAIN,
              out=None, double=True):
@@ -297,19 +311,21 @@ class Context:
 
 PS_PLAN_GRAPH = 1
 PS_PLAN_KAPPA = 2
+PS_PLAN_AUTOTUNE = 4
 
 
 class Plan:
     """ps_gpu_plan: a batch planned once, executed per field (CUDA graph replay
     with graph=True)."""
 
-    def __init__(self, ctx: Context, cfgs, method=PS_FP32_BATCHED, graph=True, kappa=False):
+    def __init__(self, ctx: Context, cfgs, method=PS_FP32_BATCHED, graph=True, kappa=False, autotune=False):
         arr = cfgs if isinstance(cfgs, C.Array) else (ps_cfg * len(cfgs))(*cfgs)
         self.ctx = ctx
         self.n = len(arr)
         self.kappa = kappa
         h = C.c_void_p()
-        flags = (PS_PLAN_GRAPH if graph else 0) | (PS_PLAN_KAPPA if kappa else 0)
+        flags = ((PS_PLAN_GRAPH if graph else 0) | (PS_PLAN_KAPPA if kappa else 0)
+                 | (PS_PLAN_AUTOTUNE if autotune else 0))
         _check(lib().ps_gpu_plan_create(ctx.handle, method, self.n, arr, flags, C.byref(h)))
         self._h = h
 

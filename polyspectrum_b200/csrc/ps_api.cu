@@ -113,6 +113,8 @@ struct ps_gpu_ctx {
     // scratch buffers replaced by larger ones stay allocated until finalize:
     // a captured plan graph may still point at them
     std::vector<void*> retired;
+    // autotuned transform size per pair-group signature (N, b_a, b_b, b_c)
+    std::map<std::array<int, 4>, int> tune_grid;
     bool capturing = false;  // inside a plan graph capture: no profiling events
     // host uploads: two staging slots of (dens, xhii), filled on copy_stream;
     // ev_copied[s] = slot s filled, ev_free[s] = its forward transform is done
@@ -131,17 +133,19 @@ struct ps_gpu_ctx {
     bool field_set = false;
     // per-kernel profiling (ps_gpu_set_profiling)
     struct ProfRec {
-        int kind;
+        int kind, size;
         cudaEvent_t a, b;
         double bytes;
+    };
+    struct ProfAgg {
+        double ms = 0.0, bytes = 0.0;
+        long long n = 0;
     };
     bool prof_on = false;
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
-    double prof_ms[32] = {0};
-    double prof_bytes[32] = {0};
-    long long prof_n[32] = {0};
+    std::map<std::pair<int, int>, ProfAgg> prof_agg;  // (family, transform size)
 };
 
 namespace {
@@ -354,7 +358,6 @@ const char* const kFamilyName[KF_COUNT] = {"fwd_z_r2c", "pass_y", "fwd_x_store",
                                            "derived_range", "finalize", "pair_z", "shell_lut", "adjoint",
                                            "pair2_parseval"};
 // families of FP64 transform kernels are counted apart (name suffix _f64)
-constexpr int KF_SLOTS = 2 * KF_COUNT;
 template <typename T> constexpr int fam(int kind) { return sizeof(T) == 8 ? kind + KF_COUNT : kind; }
 
 int prof_fold(ps_gpu_ctx* c)
@@ -364,9 +367,10 @@ int prof_fold(ps_gpu_ctx* c)
     for (const auto& r : c->prof) {
         float ms = 0.f;
         PS_CK(cudaEventElapsedTime(&ms, r.a, r.b));
-        c->prof_ms[r.kind] += ms;
-        c->prof_bytes[r.kind] += r.bytes;
-        c->prof_n[r.kind] += 1;
+        ps_gpu_ctx::ProfAgg& g = c->prof_agg[{r.kind, r.size}];
+        g.ms += ms;
+        g.bytes += r.bytes;
+        g.n += 1;
     }
     c->prof.clear();
     c->ev_used = 0;
@@ -395,7 +399,8 @@ struct Prof {
             if (a) cudaEventRecord(a, c->stream);
         }
     }
-    void end(int kind, double bytes)
+    // size: the transform size of the launch (0 for size-free kernels)
+    void end(int kind, double bytes, int size = 0)
     {
         c->launches++;
         if (!c->capturing) c->launches_total++;
@@ -403,7 +408,7 @@ struct Prof {
         cudaEvent_t b = prof_event(c);
         if (!b) return;
         cudaEventRecord(b, c->stream);
-        c->prof.push_back({kind, a, b, bytes});
+        c->prof.push_back({kind, size, a, b, bytes});
     }
 };
 
@@ -436,13 +441,13 @@ int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, i
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, dst, S, mode, dshell, N / 2 + 1, tb, quad,
                                                 c->N))));
         const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
-        pf.end(fam<T>(KF_INV_X), q * NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0));
+        pf.end(fam<T>(KF_INV_X), q * NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0), N);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, tb, quad))));
         const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
-        pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V);
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V, N);
     }
     *S_out = S;
     *hb_out = hb;
@@ -469,7 +474,7 @@ int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, co
         const double real = NN2 * N * sizeof(T);
         const double extra = (epi == EPI_STORE ? real : 0.0) + (epi == EPI_MUL_STORE ? 2.0 * real : 0.0) +
                              (epi == EPI_MUL_REDUCE ? real : 0.0);
-        pf.end(fam<T>(KF_INV_Z), NN2 * hb * V + extra);
+        pf.end(fam<T>(KF_INV_Z), NN2 * hb * V + extra, N);
     }
     if (reduce) PS_TRY(sum_partials(c, nb, 1, dsum, 1));
     PS_CK(cudaGetLastError());
@@ -493,12 +498,12 @@ int pair_spectrum(ps_gpu_ctx* c, const V2<T>* A, int Sa, int hba, const V2<T>* B
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, tb, quad))));
-        pf.end(fam<T>(KF_PAIR_Z), q * NN2 * (hba + (Bq ? hbb : 0) + hout) * V);
+        pf.end(fam<T>(KF_PAIR_Z), q * NN2 * (hba + (Bq ? hbb : 0) + hout) * V, N);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, tb, quad))));
-        pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V);
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V, N);
     }
     *S_out = S;
     return PS_OK;
@@ -517,12 +522,12 @@ int r2c_work(ps_gpu_ctx* c, int kind, const void* a, const void* b, int hout, in
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.work, S, hout, B.tables()))));
-        pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * hout * V);
+        pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * hout * V, N);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, false, B.tables()))));
-        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * S * V);
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * S * V, N);
     }
     *stride_out = S;
     return PS_OK;
@@ -539,18 +544,18 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, N / 2 + 1, B.tables()))));
-        pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * H * V);
+        pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * H * V, N);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tables()))));
-        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * B.S * V);
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * B.S * V, N);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.spec, B.S, N / 2 + 1, epi, B.spec, B.S, nullptr, 0,
                                                 nullptr, 0, nullptr, 0, nullptr, B.tables(), nullptr))));
-        pf.end(fam<T>(KF_FWD_X_STORE), 2.0 * NN2 * H * V);
+        pf.end(fam<T>(KF_FWD_X_STORE), 2.0 * NN2 * H * V, N);
     }
     PS_CK(cudaGetLastError());
     B.have_spec = true;
@@ -599,7 +604,7 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
                                                     dshells + s0, cnt, lut, lut_size, c->partials, tb, &nb,
                                                     weight, quad, c->N, (int)std::min<long long>(r2max, 0x7fffffff)))));
             const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / ((double)N * N) : 1.0;
-            pf.end(fam<T>(KF_FWD_X_DOT), q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0));
+            pf.end(fam<T>(KF_FWD_X_DOT), q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0), N);
         }
         PS_TRY(sum_partials(c, nb, cnt, dout + s0, 1));
     }
@@ -1039,13 +1044,68 @@ struct LegKey {
 // the cyclic sums over the M-grid and over the N-grid count the same triples
 // (the reference's N-grid sums then have no aliased triples either); 2 b < M
 // keeps every mode of a shell on its own M-grid index.  N when none fits.
+const int kGridSizes[] = {16, 32, 64, 128, 192, 256, 320, 384, 512, 1024};
+
 int alias_free_grid(int N, int ba, int bb, int bc)
 {
-    static const int sizes[] = {16, 32, 64, 128, 192, 256, 320, 384, 512, 1024};
     const int bmax = std::max({ba, bb, bc});
-    for (int M : sizes)
+    for (int M : kGridSizes)
         if (M < N && M > ba + bb + bc && M > 2 * bmax) return M;
     return N;
+}
+
+bool grid_supported(int M)
+{
+    for (int q : kGridSizes)
+        if (q == M) return true;
+    return false;
+}
+
+// Autotuning of a pair group's transform size: the alias-free minimum M0 and
+// up to two larger supported sizes (<= N) are each run once to warm up, then
+// timed over three runs with CUDA events on the context's stream; the fastest
+// wins.  Every candidate gives the same counts and the same sums up to FP32
+// rounding of the transforms.
+int tune_grid(ps_gpu_ctx* c, const std::function<std::function<int()>(int)>& group_op, int M0, int* best)
+{
+    std::vector<int> cands;
+    for (int q : kGridSizes)
+        if (q >= M0 && q <= c->N && cands.size() < 3) cands.push_back(q);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PS_CK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(PS_ERR_CUDA, "event creation failed");
+    }
+    float best_ms = 0.f;
+    int rc = PS_OK;
+    *best = M0;
+    for (int M : cands) {
+        if (M < c->N) {
+            Tables<float> t32;
+            Tables<double> t64;
+            if ((rc = tables_for<float>(c, M, &t32)) != PS_OK || (rc = tables_for<double>(c, M, &t64)) != PS_OK) break;
+        }
+        const auto op = group_op(M);
+        if ((rc = op()) != PS_OK) break;
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 3 && rc == PS_OK; r++) rc = op();
+        cudaEventRecord(e1, c->stream);
+        if (rc != PS_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "autotune timing failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (M == cands[0] || ms < best_ms) {
+            best_ms = ms;
+            *best = M;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
 }
 
 int sum_partials_n(ps_gpu_ctx* c, int nblocks, int ncols, double* out)
@@ -1345,6 +1405,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         });
     }
     // ---- pair groups
+    bool prefix_done = false;
     for (size_t g = 0; g < groups.size(); g++) {
         const Group G = groups[g];
         const Shell sa = host_shell_of(G.a), sb = host_shell_of(G.b);
@@ -1355,35 +1416,58 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         const int go = gofs[g], io = gidx_ofs[g];
         const Shell* hsh = table.data();  // host copy kept alive by the closure below
         std::vector<Shell> gtable(table.begin() + go, table.begin() + go + ng);
-        // the group's transforms run on the smallest M-grid on which no triple
-        // of its modes aliases (scale of the product spectrum: (N/M)^3)
-        const int M = alias_free_grid(N, std::min(sa.band, N / 2), std::min(sb.band, N / 2), hmax);
-        const double wD = ((double)N / M) * ((double)N / M) * ((double)N / M);
+        // the group's transforms run on an M-grid on which no triple of its
+        // modes aliases (scale of the product spectrum: (N/M)^3): the smallest
+        // one, or the fastest candidate when autotuned
+        const int ba = std::min(sa.band, N / 2), bb = std::min(sb.band, N / 2);
+        auto group_op = [=](int M) -> std::function<int()> {
+            const double wD = ((double)N / M) * ((double)N / M) * ((double)N / M);
+            return [=]() {
+                int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
+                // D part (FP32)
+                PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.a, sa.band, c->f.work, &Sa, &ha, 0, M));
+                if (G.a != G.b)
+                    PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.b, sb.band, c->f.work2, &Sb, &hbb, 0, M));
+                PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout,
+                                            &S, 0, M));
+                PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, dtable + go, gtable.data(), ng, gD, 0, M,
+                                       wD));
+                if (kappa)
+                    PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, dtable + go, gtable.data(), ng, gA,
+                                           0, M, wD));
+                // I part (FP64 counts on the xy-quadrant: unit filters are even in every axis)
+                PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.a, sa.band, c->d.work, &Sa, &ha, 1, M));
+                if (G.a != G.b)
+                    PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.b, sb.band, c->d.work2, &Sb, &hbb, 1, M));
+                PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout,
+                                             &S, 1, M));
+                PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, dtable + go, gtable.data(), ng, gI, 1,
+                                        M));
+                return PS_OK;
+            };
+        };
+        int M = alias_free_grid(N, ba, bb, hmax);
+        const std::array<int, 4> key = {N, ba, bb, hmax};
+        auto known = c->tune_grid.find(key);
+        if (known != c->tune_grid.end() && known->second >= M && known->second <= N && grid_supported(known->second)) {
+            M = known->second;
+        } else if (P->flags & PS_PLAN_AUTOTUNE) {
+            if (!prefix_done) {  // the DERIVED chain fills the closing shells the candidates read
+                for (auto& op : ops) PS_TRY(op());
+                prefix_done = true;
+            }
+            PS_TRY(tune_grid(c, group_op, M, &M));
+            c->tune_grid[key] = M;
+        }
         if (M < N) {
             Tables<float> t32;
             Tables<double> t64;
             PS_TRY(tables_for<float>(c, M, &t32));
             PS_TRY(tables_for<double>(c, M, &t64));
         }
+        const auto gop = group_op(M);
         ops.push_back([=]() {
-            int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
-            // D part (FP32)
-            PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.a, sa.band, c->f.work, &Sa, &ha, 0, M));
-            if (G.a != G.b)
-                PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.b, sb.band, c->f.work2, &Sb, &hbb, 0, M));
-            PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout, &S,
-                                        0, M));
-            PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, dtable + go, gtable.data(), ng, gD, 0, M, wD));
-            if (kappa)
-                PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, dtable + go, gtable.data(), ng, gA, 0,
-                                       M, wD));
-            // I part (FP64 counts on the xy-quadrant: unit filters are even in every axis)
-            PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.a, sa.band, c->d.work, &Sa, &ha, 1, M));
-            if (G.a != G.b)
-                PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.b, sb.band, c->d.work2, &Sb, &hbb, 1, M));
-            PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout, &S,
-                                         1, M));
-            PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, dtable + go, gtable.data(), ng, gI, 1, M));
+            PS_TRY(gop());
             PS_TRY(scatter_dev(c, gD, didx + io, ng, sumD));
             PS_TRY(scatter_dev(c, gI, didx + io, ng, sumI));
             if (kappa) PS_TRY(scatter_dev(c, gA, didx + io, ng, sumA));
@@ -1632,7 +1716,7 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
     if (n == 2) {
         Prof pf(c);
         k_grad_pair2<T><<<148 * 8, 256, 0, c->stream>>>(N, B.spec, B.S, c->dshells, B.hacc, B.S, hb);
-        pf.end(fam<T>(KF_GRAD), 2.0 * N * N * hb * sizeof(V2<T>));
+        pf.end(fam<T>(KF_GRAD), 2.0 * N * N * hb * sizeof(V2<T>), N);
     } else {
         // leg i: FFT of the product of the other two legs, masked by F_i;
         // identical (mask, pair) terms are folded into one with a weight
@@ -1665,7 +1749,7 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.work3, S, hout, SPEC_MASK_ADD, B.hacc, B.S, nullptr,
                                                     0, c->dshells + li, 1, nullptr, 0, nullptr, B.tables(),
                                                     nullptr, (double)tm.second))));
-            pf.end(fam<T>(KF_GRAD), 3.0 * N * N * S * sizeof(V2<T>));
+            pf.end(fam<T>(KF_GRAD), 3.0 * N * N * S * sizeof(V2<T>), N);
         }
     }
     // inverse transform of the accumulated spectrum into B.ra, then scale
@@ -1674,18 +1758,18 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.hacc, B.S, B.work, S, LOAD_PLAIN, nullptr, hb, B.tables()))));
-        pf.end(fam<T>(KF_INV_X), 2.0 * N * N * S * sizeof(V2<T>));
+        pf.end(fam<T>(KF_INV_X), 2.0 * N * N * S * sizeof(V2<T>), N);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work, S, true, B.tables()))));
-        pf.end(fam<T>(KF_PASS_Y), 2.0 * N * N * S * sizeof(V2<T>));
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * N * N * S * sizeof(V2<T>), N);
     }
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_z(c->stream, B.work, S, hb, B.ra, nullptr, EPI_STORE, 1, nullptr,
                                                 B.tables(), &nb))));
-        pf.end(fam<T>(KF_INV_Z), (double)N * N * hb * sizeof(V2<T>) + (double)n3 * sizeof(T));
+        pf.end(fam<T>(KF_INV_Z), (double)N * N * hb * sizeof(V2<T>) + (double)n3 * sizeof(T), N);
     }
     void* dst = out;
     void* stage = nullptr;
@@ -1700,7 +1784,7 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
             k_scale_out<T, double><<<148 * 8, 256, 0, c->stream>>>(B.ra, (double*)dst, n3, scale);
         else
             k_scale_out<T, float><<<148 * 8, 256, 0, c->stream>>>(B.ra, (float*)dst, n3, scale);
-        pf.end(fam<T>(KF_GRAD), (double)n3 * (sizeof(T) + (out_is_double ? 8 : 4)));
+        pf.end(fam<T>(KF_GRAD), (double)n3 * (sizeof(T) + (out_is_double ? 8 : 4)), N);
     }
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && stage) {
@@ -2085,7 +2169,7 @@ int ps_gpu_plan_create(ps_gpu_ctx* c, int method, int nconf, const ps_cfg* cfgs,
     *out = nullptr;
     if (method != PS_FP64_PLAIN && method != PS_FP32_BATCHED) return fail(PS_ERR_ARG, "method %d", method);
     if (!(c->methods & method)) return fail(PS_ERR_ARG, "method %d not enabled for this context", method);
-    if (flags & ~(PS_PLAN_GRAPH | PS_PLAN_KAPPA)) return fail(PS_ERR_ARG, "flags %d", flags);
+    if (flags & ~(PS_PLAN_GRAPH | PS_PLAN_KAPPA | PS_PLAN_AUTOTUNE)) return fail(PS_ERR_ARG, "flags %d", flags);
     PS_CK(cudaSetDevice(c->device));
     ps_gpu_plan* P = new ps_gpu_plan();
     P->ctx = c;
@@ -2178,15 +2262,54 @@ int ps_gpu_synchronize(ps_gpu_ctx* c)
 
 long long ps_gpu_launch_count(ps_gpu_ctx* c) { return c ? c->launches_total : -1; }
 
+int ps_gpu_tune_export(ps_gpu_ctx* c, char* buf, int buflen)
+{
+    g_err[0] = 0;
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    std::string t;
+    char line[96];
+    for (const auto& kv : c->tune_grid) {
+        snprintf(line, sizeof(line), "grid %d %d %d %d %d\n", kv.first[0], kv.first[1], kv.first[2], kv.first[3],
+                 kv.second);
+        t += line;
+    }
+    if (buf && buflen > 0) {
+        const size_t n = std::min(t.size(), (size_t)buflen - 1);
+        memcpy(buf, t.data(), n);
+        buf[n] = '\0';
+    }
+    return (int)t.size();
+}
+
+int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
+{
+    g_err[0] = 0;
+    if (!c || !text) return fail(PS_ERR_ARG, "NULL argument");
+    std::map<std::array<int, 4>, int> add;
+    const char* p = text;
+    while (*p) {
+        const char* e = strchr(p, '\n');
+        const std::string ln(p, e ? (size_t)(e - p) : strlen(p));
+        p = e ? e + 1 : p + ln.size();
+        if (ln.find_first_not_of(" \t\r") == std::string::npos) continue;
+        int n, ba, bb, bc, m, used = 0;
+        if (sscanf(ln.c_str(), "grid %d %d %d %d %d %n", &n, &ba, &bb, &bc, &m, &used) != 5 ||
+            ln.find_first_not_of(" \t\r", used) != std::string::npos)
+            return fail(PS_ERR_ARG, "tune line not understood: '%s'", ln.c_str());
+        if (!grid_supported(m) || m > n || ba < 0 || bb < 0 || bc < 0)
+            return fail(PS_ERR_ARG, "tune line out of range: '%s'", ln.c_str());
+        add[{n, ba, bb, bc}] = m;
+    }
+    for (const auto& kv : add) c->tune_grid[kv.first] = kv.second;
+    return PS_OK;
+}
+
 int ps_gpu_set_profiling(ps_gpu_ctx* c, int on)
 {
     if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
     PS_TRY(prof_fold(c));
     if (on && !c->prof_on) {
-        for (int q = 0; q < KF_SLOTS; q++) {
-            c->prof_ms[q] = c->prof_bytes[q] = 0.0;
-            c->prof_n[q] = 0;
-        }
+        c->prof_agg.clear();
     }
     c->prof_on = on != 0;
     return PS_OK;
@@ -2198,15 +2321,17 @@ int ps_gpu_kernel_stats(ps_gpu_ctx* c, ps_kernel_stat* out, int max)
     PS_CK(cudaSetDevice(c->device));
     PS_TRY(prof_fold(c));
     int cnt = 0;
-    for (int q = 0; q < KF_SLOTS; q++) {
-        if (!c->prof_n[q]) continue;
+    for (const auto& kv : c->prof_agg) {
+        const int q = kv.first.first, size = kv.first.second;
         if (out && cnt < max) {
             memset(&out[cnt], 0, sizeof(ps_kernel_stat));
-            snprintf(out[cnt].name, sizeof(out[cnt].name), "%s%s", kFamilyName[q % KF_COUNT],
-                     q >= KF_COUNT ? "_f64" : "");
-            out[cnt].launches = c->prof_n[q];
-            out[cnt].ms = c->prof_ms[q];
-            out[cnt].bytes = c->prof_bytes[q];
+            char sz[16] = "";
+            if (size > 0) snprintf(sz, sizeof(sz), "@%d", size);
+            snprintf(out[cnt].name, sizeof(out[cnt].name), "%s%s%s", kFamilyName[q % KF_COUNT],
+                     q >= KF_COUNT ? "_f64" : "", sz);
+            out[cnt].launches = kv.second.n;
+            out[cnt].ms = kv.second.ms;
+            out[cnt].bytes = kv.second.bytes;
         }
         cnt++;
     }

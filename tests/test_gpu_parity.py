@@ -316,3 +316,42 @@ def test_mixed_radix_subgrids_match_plain(gpu_lib, n_grid, pairs):
     for i in range(len(cfgs)):
         assert list(out32[i].kmin)[:3] == list(out64[i].kmin)[:3]
         assert list(out32[i].kmax)[:3] == list(out64[i].kmax)[:3]
+
+
+def test_autotuned_plan_and_tune_table(gpu_lib):
+    """An autotuned plan (transform size per pair group picked by timing) keeps
+    counts and derived ranges identical and B within the batched tolerance of
+    plain FP64; its choices exported from one context and imported into
+    another reproduce its results bit for bit without timing."""
+    from polyspectrum_b200 import synth
+    ps = gpu_lib
+    n_grid, box = 256, 400.0
+    dens, xhii = synth.xhi_dens_inputs(n_grid, box, 4000, 3, 2.0, 4)
+    cfgs = []
+    for k1, k2 in ((0.2, 0.5), (0.5, 0.8), (0.8, 1.2)):
+        c, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1, k2=k2, num_values=8, kbinningCase=1)
+        cfgs += [c[i] for i in range(len(c))]
+    with ps.Context(n_grid, box) as ctx:
+        ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+        plan = ctx.plan(cfgs, autotune=True)
+        Bt, Nt, _, outt = plan.execute()
+        plan.close()
+        B64, N64, _, out64 = ctx.batch(cfgs, ps.PS_FP64_PLAIN)
+        table = ctx.tune_export()
+    assert table.count("grid ") >= 2, table
+    scale = np.abs(B64).max()
+    assert np.all(np.abs(Bt - B64) <= 1e-5 * np.abs(B64) + 1e-6 * scale)
+    np.testing.assert_array_equal(Nt, np.rint(N64))
+    for i in range(len(cfgs)):
+        assert list(outt[i].kmin)[:3] == list(out64[i].kmin)[:3]
+    with ps.Context(n_grid, box) as ctx2:
+        ctx2.tune_import(table)
+        assert ctx2.tune_export() == table
+        ctx2.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+        plan2 = ctx2.plan(cfgs)
+        B2, N2, _, _ = plan2.execute()
+        plan2.close()
+        with pytest.raises(ps.PsError):
+            ctx2.tune_import("grid 256 1 2 three 64\n")
+    np.testing.assert_array_equal(B2, Bt)
+    np.testing.assert_array_equal(N2, Nt)
