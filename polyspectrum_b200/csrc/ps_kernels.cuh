@@ -614,8 +614,17 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
                     const double m = hypot(v.x, v.y);
                     v = V{v.x / m, v.y / m};
                 } else {
-                    const float m = hypotf(v.x, v.y);
-                    v = V{v.x / m, v.y / m};
+                    // FP32 spectra: one reciprocal square root when |v|^2 is a
+                    // normal float, the overflow-safe quotient otherwise (a zero
+                    // mode stays 0/0 = NaN, as utils_fftw.c:89 gives)
+                    const float m2 = v.x * v.x + v.y * v.y;
+                    if (m2 >= 1.17549435e-38f && m2 <= 3.40282347e38f) {
+                        const float r = rsqrtf(m2);
+                        v = V{v.x * r, v.y * r};
+                    } else {
+                        const float m = hypotf(v.x, v.y);
+                        v = V{v.x / m, v.y / m};
+                    }
                 }
             } else if (epi == SPEC_MASK_ADD) {
                 if (!((keep >> e) & 1u)) continue;
