@@ -195,10 +195,18 @@ long long ps_gpu_launch_count(ps_gpu_ctx *ctx);
 /* Gradient dB/d(delta) of one configuration with respect to the real input
  * field (the array the forward transform read), written to out as N^3 float
  * (out_is_double = 0) or double (1) in host or device memory (out_mem).  No
- * reference counterpart; defined for use_only_phase = 0. */
+ * reference counterpart.  For a phase-only field (use_only_phase = 1) the
+ * gradient goes through z/|z| and needs the modulus kept at loading
+ * (ps_gpu_keep_modulus); without it PS_ERR_UNSUPPORTED. */
 int ps_gpu_grad(ps_gpu_ctx *ctx, int method, int n, const double *k, const double *kmin,
                 const double *kmax, double kbinwidth, int kbinningCase, void *out,
                 int out_is_double, int out_mem);
+
+/* With on != 0, later phase-only loads (use_only_phase = 1) also keep |X| per
+ * mode of the field spectrum (one more real half-spectrum on the device), which
+ * ps_gpu_grad needs to differentiate through z/|z| (utils_fftw.c:78-93).  No
+ * reference counterpart. */
+int ps_gpu_keep_modulus(ps_gpu_ctx *ctx, int on);
 
 /* The configuration list of a run: read_params_to_kvectors (kvectors.c:46-147)
  * plus the per-configuration kpolygon bookkeeping of run.c:56-84.  Writes at

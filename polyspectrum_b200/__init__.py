@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
     L.ps_gpu_launch_count.argtypes = [vp]
     L.ps_gpu_launch_count.restype = C.c_longlong
     L.ps_gpu_tune_export.argtypes = [vp, C.c_char_p, ip]
+    L.ps_gpu_keep_modulus.argtypes = [vp, ip]
     L.ps_gpu_tune_import.argtypes = [vp, C.c_char_p]
     L.ps_gpu_set_profiling.argtypes = [vp, ip]
     L.ps_gpu_kernel_stats.argtypes = [vp, C.POINTER(ps_kernel_stat), ip]
@@ -103,7 +104,7 @@ def lib() -> C.CDLL:
                  "ps_gpu_set_stream", "ps_gpu_last_timing", "ps_gpu_set_profiling",
                  "ps_gpu_kernel_stats", "ps_gpu_plan_create", "ps_gpu_plan_execute",
                  "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize",
-                 "ps_gpu_tune_export", "ps_gpu_tune_import"):
+                 "ps_gpu_tune_export", "ps_gpu_tune_import", "ps_gpu_keep_modulus"):
         getattr(L, name).restype = ip
     _lib = L
     return L
@@ -266,6 +267,10 @@ class Context:
              autotune: bool = False):
         """A reusable plan of these configurations (ps_gpu_plan_create)."""
         return Plan(self, cfgs, method, graph, kappa, autotune)
+
+    def keep_modulus(self, on: bool = True):
+        """Phase-only loads keep |X| so grad() can differentiate through z/|z|."""
+        _check(lib().ps_gpu_keep_modulus(self._h, int(bool(on))))
 
     def tune_export(self) -> str:
         """The autotuned sub-grid choices of this context (ps_gpu_tune_export)."""

@@ -85,8 +85,10 @@ template <typename T> struct PrecBufs {
     V2<T>* hacc = nullptr;  // adjoint spectrum accumulator (allocated on use)
     T* ra = nullptr;        // real grids
     T* rb = nullptr;
+    T* mod = nullptr;       // |X| of a phase-only field (ps_gpu_keep_modulus)
     int S = 0;
     bool have_spec = false;
+    bool have_mod = false;
     // tables of smaller transform sizes (sub-grid products), made at plan time
     std::map<int, std::array<V2<T>*, 3>> sub;
 };
@@ -130,6 +132,7 @@ struct ps_gpu_ctx {
     long long launches = 0;
     long long launches_total = 0;  // kernels executed since creation (graph replays included)
     int use_only_phase = 0;
+    bool keep_modulus = false;  // phase-only loads keep |X| (phase-only adjoint)
     bool field_set = false;
     // per-kernel profiling (ps_gpu_set_profiling)
     struct ProfRec {
@@ -267,6 +270,7 @@ template <typename T> void free_prec(PrecBufs<T>& b)
     cudaFree(b.work2);
     cudaFree(b.work3);
     cudaFree(b.hacc);
+    cudaFree(b.mod);
     cudaFree(b.ra);
     cudaFree(b.rb);
     b = PrecBufs<T>();
@@ -539,6 +543,12 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
     const int epi = c->use_only_phase == 1 ? SPEC_STORE_PHASE : SPEC_STORE;
+    T* mod = nullptr;
+    B.have_mod = false;
+    if (epi == SPEC_STORE_PHASE && c->keep_modulus) {
+        PS_TRY(alloc_dev(&B.mod, (size_t)N * N * B.S));
+        mod = B.mod;
+    }
     const double V = sizeof(V2<T>), NN2 = (double)N * N, H = N / 2 + 1;
     const double src_bytes = kind == SRC_F32 ? 4.0 : kind == SRC_F64 ? 8.0 : kind == SRC_XHI_F32 ? 8.0 : 16.0;
     {
@@ -554,11 +564,13 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.spec, B.S, N / 2 + 1, epi, B.spec, B.S, nullptr, 0,
-                                                nullptr, 0, nullptr, 0, nullptr, B.tables(), nullptr))));
+                                                nullptr, 0, nullptr, 0, nullptr, B.tables(), nullptr, 1.0, 0, 0,
+                                                0x7fffffff, mod))));
         pf.end(fam<T>(KF_FWD_X_STORE), 2.0 * NN2 * H * V, N);
     }
     PS_CK(cudaGetLastError());
     B.have_spec = true;
+    B.have_mod = mod != nullptr;
     return PS_OK;
 }
 
@@ -1752,6 +1764,11 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
             pf.end(fam<T>(KF_GRAD), 3.0 * N * N * S * sizeof(V2<T>), N);
         }
     }
+    if (c->use_only_phase == 1) {  // the field entered through z/|z|
+        Prof pf(c);
+        k_phase_adjoint<T><<<148 * 8, 256, 0, c->stream>>>((size_t)N * N, hb, B.hacc, B.S, B.spec, B.mod);
+        pf.end(fam<T>(KF_GRAD), 4.0 * N * N * hb * sizeof(V2<T>), N);
+    }
     // inverse transform of the accumulated spectrum into B.ra, then scale
     const int S = round_up(hb, pw<T>(N));
     int nb = 0;
@@ -2037,9 +2054,9 @@ int ps_gpu_grad(ps_gpu_ctx* c, int method, int n, const double* k, const double*
     if (out_mem != PS_MEM_HOST && out_mem != PS_MEM_DEVICE) return fail(PS_ERR_ARG, "out_mem=%d", out_mem);
     if (n != 2 && n != 3)
         return fail(PS_ERR_UNSUPPORTED, "ps_gpu_grad: n=%d (the reference's configurations have n = 2 or 3)", n);
-    if (c->use_only_phase == 1)
-        return fail(PS_ERR_UNSUPPORTED, "ps_gpu_grad: the field was loaded phase-only; the gradient is defined "
-                                        "for use_only_phase = 0");
+    if (c->use_only_phase == 1 && !(method == PS_FP64_PLAIN ? c->d.have_mod : c->f.have_mod))
+        return fail(PS_ERR_UNSUPPORTED, "ps_gpu_grad: the field was loaded phase-only without its modulus; call "
+                                        "ps_gpu_keep_modulus(ctx, 1) before loading it");
     PS_CK(cudaSetDevice(c->device));
     ps_cfg g;
     memset(&g, 0, sizeof(g));
@@ -2261,6 +2278,14 @@ int ps_gpu_synchronize(ps_gpu_ctx* c)
 }
 
 long long ps_gpu_launch_count(ps_gpu_ctx* c) { return c ? c->launches_total : -1; }
+
+int ps_gpu_keep_modulus(ps_gpu_ctx* c, int on)
+{
+    g_err[0] = 0;
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    c->keep_modulus = on != 0;
+    return PS_OK;
+}
 
 int ps_gpu_tune_export(ps_gpu_ctx* c, char* buf, int buflen)
 {

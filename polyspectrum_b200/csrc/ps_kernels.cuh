@@ -428,11 +428,38 @@ __device__ __forceinline__ T load_real(int kind, const void* a, const void* b, s
     }
 }
 
-// One tile per CTA (the input rows are dense and all loads are issued up front).
+// Real values 2n and 2n+1 of a row (ra, and rb for XHI_DENS), composed as
+// load_real does, with one vector load per array.
+template <typename T>
+__device__ __forceinline__ V2<T> load_pair(int kind, const unsigned char* ra, const unsigned char* rb, int n)
+{
+    switch (kind) {
+    case SRC_F32: {
+        const float2 v = reinterpret_cast<const float2*>(ra)[n];
+        return V2<T>{(T)v.x, (T)v.y};
+    }
+    case SRC_F64: {
+        const double2 v = reinterpret_cast<const double2*>(ra)[n];
+        return V2<T>{(T)v.x, (T)v.y};
+    }
+    case SRC_XHI_F32: {
+        const float2 d = reinterpret_cast<const float2*>(ra)[n], x = reinterpret_cast<const float2*>(rb)[n];
+        return V2<T>{(T)__dmul_rn((double)d.x, __dsub_rn(1.0, (double)x.x)),
+                     (T)__dmul_rn((double)d.y, __dsub_rn(1.0, (double)x.y))};
+    }
+    default: {  // SRC_XHI_F64
+        const double2 d = reinterpret_cast<const double2*>(ra)[n], x = reinterpret_cast<const double2*>(rb)[n];
+        return V2<T>{(T)__dmul_rn(d.x, __dsub_rn(1.0, x.x)), (T)__dmul_rn(d.y, __dsub_rn(1.0, x.y))};
+    }
+    }
+}
+
+// One tile per CTA (the input rows are dense and all loads are issued up front;
+// `vec`: the sources are aligned for one vector load per value pair).
 template <typename T, int N>
 __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
     k_fwd_z(int kind, const void* __restrict__ a_src, const void* __restrict__ b_src,
-            V2<T>* __restrict__ dst, int dst_stride, int hout, const V2<T>* __restrict__ twr_g,
+            V2<T>* __restrict__ dst, int dst_stride, int hout, int vec, const V2<T>* __restrict__ twr_g,
             const V2<T>* __restrict__ twpp_g)
 {
     using G = RowGeom<T, N>;
@@ -445,6 +472,13 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
         const V* xr = reinterpret_cast<const V*>((const T*)a_src + row * N);
 #pragma unroll
         for (int e = 0; e < G::R; e++) a[e] = xr[t0 + G::TPF * e];
+    } else if (vec) {
+        // both values of a pair in one 8- or 16-byte load per array
+        const int eb = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 4 : 8;
+        const unsigned char* ra = reinterpret_cast<const unsigned char*>(a_src) + row * N * eb;
+        const unsigned char* rb = b_src ? reinterpret_cast<const unsigned char*>(b_src) + row * N * eb : nullptr;
+#pragma unroll
+        for (int e = 0; e < G::R; e++) a[e] = load_pair<T>(kind, ra, rb, t0 + G::TPF * e);
     } else {
 #pragma unroll
         for (int e = 0; e < G::R; e++) {
@@ -537,7 +571,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, int ndk, const Shell* __restrict__ shells,
             int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight, int quad,
-            int r2max, double* __restrict__ partials, const V2<T>* __restrict__ tw_g)
+            int r2max, double* __restrict__ partials, const V2<T>* __restrict__ tw_g, T* __restrict__ mod_out)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
@@ -610,8 +644,10 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
             const int i = t + G::TPF * e;
             V v = a[e];
             if (epi == SPEC_STORE_PHASE) {
+                // mod_out (optional) keeps |X| for the phase-only adjoint
+                T m;
                 if constexpr (sizeof(T) == 8) {
-                    const double m = hypot(v.x, v.y);
+                    m = hypot(v.x, v.y);
                     v = V{v.x / m, v.y / m};
                 } else {
                     // FP32 spectra: one reciprocal square root when |v|^2 is a
@@ -621,11 +657,13 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
                     if (m2 >= 1.17549435e-38f && m2 <= 3.40282347e38f) {
                         const float r = rsqrtf(m2);
                         v = V{v.x * r, v.y * r};
+                        m = m2 * r;
                     } else {
-                        const float m = hypotf(v.x, v.y);
+                        m = hypotf(v.x, v.y);
                         v = V{v.x / m, v.y / m};
                     }
                 }
+                if (mod_out) mod_out[((size_t)i * N + j) * out_stride + h] = m;
             } else if (epi == SPEC_MASK_ADD) {
                 if (!((keep >> e) & 1u)) continue;
                 V* o = out + ((size_t)i * N + j) * out_stride + h;
@@ -721,6 +759,26 @@ __global__ void k_grad_pair2(int n, const V2<T>* __restrict__ dk, int dks, const
             v = V2<T>{f * d.x, f * d.y};
         }
         hacc[r * S + h] = v;
+    }
+}
+
+// Phase-only adjoint: the field enters through phi = z/|z| per mode, whose
+// differential is (dz - phi Re(conj(phi) dz)) / |z|; its transpose maps the
+// accumulated gradient spectrum H to (H - phi Re(conj(phi) H)) / |z| (in
+// place, rows of the half spectrum, h < hb).  Modes with H = 0 stay 0.
+template <typename T>
+__global__ void k_phase_adjoint(size_t rows, int hb, V2<T>* __restrict__ hacc, int S,
+                                const V2<T>* __restrict__ phi, const T* __restrict__ mod)
+{
+    const size_t total = rows * (size_t)hb;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = q / hb, idx = r * S + q % hb;
+        const V2<T> H = hacc[idx];
+        if (H.x == (T)0 && H.y == (T)0) continue;
+        const V2<T> u = phi[idx];
+        const T m = mod[idx];
+        const T p = u.x * H.x + u.y * H.y;  // Re(conj(phi) H)
+        hacc[idx] = V2<T>{(H.x - u.x * p) / m, (H.y - u.y * p) / m};
     }
 }
 

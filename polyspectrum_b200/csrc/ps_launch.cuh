@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 
 #include "../../include/ps_gpu.h"
 #include "ps_kernels.cuh"
@@ -113,7 +114,10 @@ template <typename T, int N> struct L3 {
         constexpr size_t smem = RG::STAGE_OFF;
         PS_LTRY(set_smem(k_fwd_z<T, N>, smem));
         const unsigned blocks = (unsigned)((size_t)N * N / RG::WZ);
-        k_fwd_z<T, N><<<blocks, RG::THREADS, smem, st>>>(kind, a, b, dst, ds, hout, tb.twr, tb.twpp);
+        const bool two = kind == SRC_XHI_F32 || kind == SRC_XHI_F64;
+        const uintptr_t need = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 8 : 16;  // float2 / double2
+        const int vec = kind != SRC_T && (((uintptr_t)a | (two ? (uintptr_t)b : 0)) % need) == 0;
+        k_fwd_z<T, N><<<blocks, RG::THREADS, smem, st>>>(kind, a, b, dst, ds, hout, vec, tb.twr, tb.twpp);
         return PS_OK;
     }
     static int pair_z(cudaStream_t st, const V* a, int sa, int hva, const V* b, int sb, int hvb, V* dst,
@@ -133,7 +137,7 @@ template <typename T, int N> struct L3 {
     static int fwd_x(cudaStream_t st, V* data, int stride, int hvalid, int epi, V* out, int ostride,
                      const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
                      int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0,
-                     int quad = 0, int ndk = 0, int r2max = 0x7fffffff)
+                     int quad = 0, int ndk = 0, int r2max = 0x7fffffff, T* mod_out = nullptr)
     {
         const int nj = quad ? N / 2 + 1 : N;
         const unsigned blocks = (unsigned)(nj * (stride / PG::W));
@@ -142,12 +146,12 @@ template <typename T, int N> struct L3 {
             PS_LTRY(set_smem(k_fwd_x<T, N, true>, PG::SMEM));
             k_fwd_x<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(
                 data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
-                weight, quad, r2max, partials, tb.twp);
+                weight, quad, r2max, partials, tb.twp, mod_out);
         } else {
             PS_LTRY(set_smem(k_fwd_x<T, N, false>, PG::SMEM));
             k_fwd_x<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(
                 data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
-                weight, quad, r2max, partials, tb.twp);
+                weight, quad, r2max, partials, tb.twp, mod_out);
         }
         if (nblocks) *nblocks = (int)blocks;
         return PS_OK;

@@ -132,3 +132,90 @@ def test_grad_config4_256(gpu_lib):
     with ps.Context(n_grid, box, methods=ps.PS_FP32_BATCHED) as ctx:
         g32 = _grad(ps, ctx, field, cfg, ps.PS_FP32_BATCHED, double=False)
     assert np.abs(g32 - g64).max() <= 1e-4 * np.abs(g64).max()
+
+
+def _fd_check_phase(ps, n_grid, box, cfg, nvox=12, ndir=4, field_seed=5):
+    """Phase-only field: the gradient through z/|z| against central differences."""
+    field = synth.lognormal_density(n_grid, 2.0, field_seed).astype(np.float64)
+    with ps.Context(n_grid, box, methods=ps.PS_FP64_PLAIN) as ctx:
+        ctx.keep_modulus(True)
+
+        def B(f):
+            ctx.get_FT_field(ps.PS_FIELD_DENS, f, use_only_phase=1)
+            return ctx.batch([cfg], 1)[0][0]
+        ctx.get_FT_field(ps.PS_FIELD_DENS, field, use_only_phase=1)
+        n = cfg.n
+        g = ctx.grad(n, [cfg.k[i] for i in range(n)], [cfg.kmin[i] for i in range(n)],
+                     [cfg.kmax[i] for i in range(n)], cfg.kbinwidth, cfg.kbinningCase, method=1)
+        gmax = np.abs(g).max()
+        assert gmax > 0
+        rng = np.random.default_rng(6)
+        for v in rng.integers(0, n_grid, size=(nvox, 3)):
+            fp, fm = field.copy(), field.copy()
+            fp[tuple(v)] += EPS
+            fm[tuple(v)] -= EPS
+            fd = (B(fp) - B(fm)) / (2 * EPS)
+            assert abs(fd - g[tuple(v)]) <= 1e-4 * gmax, (v, fd, g[tuple(v)], gmax)
+        rng = np.random.default_rng(7)
+        for _ in range(ndir):
+            d = rng.standard_normal(field.shape)
+            d /= np.linalg.norm(d)
+            fd = (B(field + EPS * d) - B(field - EPS * d)) / (2 * EPS)
+            an = float((g * d).sum())
+            assert abs(fd - an) <= 1e-4 * max(abs(an), 1e-300) + 1e-6 * gmax, (fd, an)
+    return g
+
+
+@pytest.mark.parametrize("kb", [0, 1])
+def test_grad_phase_only_fd(gpu_lib, kb):
+    ps = gpu_lib
+    n_grid, box = 32, 100.0
+    kf = 2 * np.pi / box
+    cfgs, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=3.2 * kf, k2=4.1 * kf, num_values=5,
+                                            kbinningCase=kb)
+    _fd_check_phase(ps, n_grid, box, cfgs[2])
+
+
+def test_grad_phase_only_power_is_zero(gpu_lib):
+    """Phase-only, n = 2: every mode has |phi|^2 = 1, so P(k) does not depend on
+    the field and its gradient vanishes (rounding residue only)."""
+    ps = gpu_lib
+    n_grid, box = 32, 100.0
+    kf = 2 * np.pi / box
+    field = synth.lognormal_density(n_grid, 2.0, 5).astype(np.float64)
+    cfg = ps.make_cfg(2, [5.0 * kf] * 2, kbinwidth=1.0)
+    with ps.Context(n_grid, box, methods=ps.PS_FP64_PLAIN) as ctx:
+        ctx.keep_modulus(True)
+        ctx.get_FT_field(ps.PS_FIELD_DENS, field, use_only_phase=1)
+        B = ctx.batch([cfg], 1)[0][0]
+        g = ctx.grad(2, [5.0 * kf] * 2, [0, 0], [0, 0], 1.0, 0, method=1)
+    d = np.random.default_rng(3).standard_normal(field.shape)
+    d *= np.linalg.norm(field) / np.linalg.norm(d)
+    # a change of the field as large as the field itself moves B by ~0
+    assert abs(float((g * d).sum())) <= 1e-9 * abs(B), (float((g * d).sum()), B)
+
+
+def test_grad_phase_only_fp32_and_torch(gpu_lib):
+    """FP32 phase-only gradient against FP64, and the torch binding with
+    use_only_phase = 1 against the C-ABI gradient."""
+    import torch
+
+    from polyspectrum_b200.autograd import polyspectrum
+    ps = gpu_lib
+    n_grid, box = 32, 100.0
+    kf = 2 * np.pi / box
+    cfg = ps.make_cfg(3, [3.3 * kf, 4.0 * kf, 5.1 * kf], kbinwidth=1.0)
+    field = synth.lognormal_density(n_grid, 2.0, 3).astype(np.float64)
+    grads = []
+    for method, dbl in ((ps.PS_FP64_PLAIN, True), (ps.PS_FP32_BATCHED, False)):
+        with ps.Context(n_grid, box, methods=method) as ctx:
+            ctx.keep_modulus(True)
+            ctx.get_FT_field(ps.PS_FIELD_DENS, field.astype(np.float64 if dbl else np.float32), use_only_phase=1)
+            grads.append(ctx.grad(3, list(cfg.k)[:3], list(cfg.kmin)[:3], list(cfg.kmax)[:3], 1.0, 0,
+                                  method=method, double=dbl))
+    assert np.abs(grads[1] - grads[0]).max() <= 1e-4 * np.abs(grads[0]).max()
+    f = torch.from_numpy(field).cuda().requires_grad_(True)
+    with ps.Context(n_grid, box, methods=ps.PS_FP64_PLAIN) as ctx:
+        B = polyspectrum(f, ctx, cfg, use_only_phase=1)
+        B.backward()
+    np.testing.assert_allclose(f.grad.cpu().numpy(), grads[0], rtol=0, atol=1e-12 * np.abs(grads[0]).max())

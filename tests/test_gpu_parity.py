@@ -355,3 +355,34 @@ def test_autotuned_plan_and_tune_table(gpu_lib):
             ctx2.tune_import("grid 256 1 2 three 64\n")
     np.testing.assert_array_equal(B2, Bt)
     np.testing.assert_array_equal(N2, Nt)
+
+
+@pytest.mark.parametrize("legs", [(3.1, 4.2, 3.7, 5.0), (4.0, 4.0, 4.0, 4.0), (2.9, 3.6, 4.4, 3.1, 5.2)],
+                         ids=["n4", "n4_equal", "n5"])
+def test_higher_polygons_match_oracle(gpu_lib, ora, legs):
+    """n = 4 and 5 (the estimator takes any n, polyspectrum.c:72; only the
+    reference's configuration generator stops at 3): both methods against the
+    oracle's polyspectrum() / num_polygons() for DEFAULT binning, with a
+    repeated shell folded into a power."""
+    ps = gpu_lib
+    n_grid, box = 32, 100.0
+    kf = 2 * np.pi / box
+    dens, _ = fields(n_grid, box)
+    L = float(np.float32(box))
+    k = np.array(legs) * kf
+    n = len(k)
+    dk = ora.ora_forward(n_grid, 0, dens)
+    lo = np.zeros(n)
+    hi = np.zeros(n)
+    b_ref, _, _, _, _ = ora.ora_polyspectrum(n_grid, dk, k, lo, hi, 1.0, 0, L)
+    n_ref = ora.ora_num_polygons(n_grid, k, lo, hi, 1.0, 0, L)
+    assert n_ref > 0
+    cfg = ps.make_cfg(n, list(k), kbinwidth=1.0)
+    with ps.Context(n_grid, box) as ctx:
+        ctx.get_FT_field(0, dens)
+        B64, N64, _, _ = ctx.batch([cfg], ps.PS_FP64_PLAIN)
+        B32, N32, _, _ = ctx.batch([cfg], ps.PS_FP32_BATCHED)
+    assert abs(B64[0] - b_ref) <= 1e-9 * abs(b_ref)
+    assert abs(N64[0] - n_ref) <= 1e-7 * max(1.0, n_ref)
+    assert abs(B32[0] - b_ref) <= 1e-5 * abs(b_ref)
+    assert N32[0] == np.rint(n_ref)
