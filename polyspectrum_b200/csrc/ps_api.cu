@@ -100,6 +100,15 @@ struct ps_gpu_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    // side lane: the count (FP64) parts of pair groups run on their own stream
+    // with their own partial sums and shell table, concurrently with the field
+    // (FP32) parts; ev_fork / ev_join order it inside a launch sequence
+    cudaStream_t side_stream = nullptr;
+    double* side_partials = nullptr;
+    size_t side_partials_cap = 0;
+    unsigned short* side_lut = nullptr;
+    size_t side_lut_cap = 0;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     PrecBufs<float> f;
     PrecBufs<double> d;
     double* partials = nullptr;
@@ -324,6 +333,22 @@ int ensure_lut(ps_gpu_ctx* c, size_t n)
     c->dlut_cap = n;
     return PS_OK;
 }
+// While alive, the context's stream, partial sums and shell table are those
+// of the side lane (every launch helper then works on the side lane).
+struct SideLane {
+    ps_gpu_ctx* c;
+    explicit SideLane(ps_gpu_ctx* cc) : c(cc) { swap(); }
+    ~SideLane() { swap(); }
+    void swap()
+    {
+        std::swap(c->stream, c->side_stream);
+        std::swap(c->partials, c->side_partials);
+        std::swap(c->partials_cap, c->side_partials_cap);
+        std::swap(c->dlut, c->side_lut);
+        std::swap(c->dlut_cap, c->side_lut_cap);
+    }
+};
+
 int ensure_minmax(ps_gpu_ctx* c, size_t n)
 {
     if (n <= c->dminmax_cap) return PS_OK;
@@ -416,10 +441,10 @@ struct Prof {
     }
 };
 
-int sum_partials(ps_gpu_ctx* c, int nblocks, int ncols, double* out, int out_stride)
+int sum_partials(ps_gpu_ctx* c, int nblocks, int ncols, double* out, int out_stride, const int* idx = nullptr)
 {
     Prof pf(c);
-    k_sum_partials<<<ncols, 1024, 0, c->stream>>>(c->partials, nblocks, out, out_stride);
+    k_sum_partials<<<ncols, 1024, 0, c->stream>>>(c->partials, nblocks, out, out_stride, idx);
     pf.end(KF_SUM, 8.0 * nblocks * ncols);
     return PS_OK;
 }
@@ -443,13 +468,13 @@ int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, i
     {
         Prof pf(c);
         PS_SWITCH_N(N, PS_TRY((L3<T, NN>::inv_x(c->stream, B.spec, B.S, dst, S, mode, dshell, N / 2 + 1, tb, quad,
-                                                c->N))));
+                                                c->N, 1))));
         const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
         pf.end(fam<T>(KF_INV_X), q * NN2 * S * V + (mode == LOAD_MASKED ? NN2 * hb * V : 0.0), N);
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, tb, quad))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, tb, quad, std::min(band, N / 2)))));
         const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
         pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V, N);
     }
@@ -580,7 +605,8 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
 // M > 0: the buffer is an M-grid spectrum; dot sums are scaled by `weight`.
 template <typename T>
 int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell* dshells,
-             const Shell* hsh, int ns, double* dout, int quad = 0, int M = 0, double weight = 1.0)
+             const Shell* hsh, int ns, double* dout, int quad = 0, int M = 0, double weight = 1.0,
+             const int* didx = nullptr)
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = M > 0 ? M : c->N;
@@ -618,7 +644,7 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
             const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / ((double)N * N) : 1.0;
             pf.end(fam<T>(KF_FWD_X_DOT), q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0), N);
         }
-        PS_TRY(sum_partials(c, nb, cnt, dout + s0, 1));
+        PS_TRY(didx ? sum_partials(c, nb, cnt, dout, 1, didx + s0) : sum_partials(c, nb, cnt, dout + s0, 1));
     }
     PS_CK(cudaGetLastError());
     return PS_OK;
@@ -1374,9 +1400,15 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
     }
     {
         const size_t pen32 = (size_t)N * (c->f.S / pw<float>(N)), pen64 = (size_t)N * (c->d.S / pw<double>(N));
-        PS_TRY(ensure_partials(c, std::max({(size_t)N * N, pen32 * MAX_DOT_SHELLS, pen64 * MAX_DOT_SHELLS,
-                                            (size_t)148 * 8 * 2 * MAX_DOT_SHELLS})));
+        const size_t np = std::max({(size_t)N * N, pen32 * MAX_DOT_SHELLS, pen64 * MAX_DOT_SHELLS,
+                                    (size_t)148 * 8 * 2 * MAX_DOT_SHELLS});
+        PS_TRY(ensure_partials(c, np));
         PS_TRY(ensure_lut(c, (size_t)3 * (N / 2) * (N / 2) + 2));
+        if (!groups.empty()) {
+            SideLane lane(c);
+            PS_TRY(ensure_partials(c, np));
+            PS_TRY(ensure_lut(c, (size_t)3 * (N / 2) * (N / 2) + 2));
+        }
     }
     const double n3 = (double)N * (double)N * (double)N;
     const double pi = ref_pi();
@@ -1432,30 +1464,43 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         // modes aliases (scale of the product spectrum: (N/M)^3): the smallest
         // one, or the fastest candidate when autotuned
         const int ba = std::min(sa.band, N / 2), bb = std::min(sb.band, N / 2);
-        auto group_op = [=](int M) -> std::function<int()> {
+        // D part (FP32 field products) and I part (FP64 counts on the xy-quadrant:
+        // unit filters are even in every axis) of the group on an M-grid
+        auto d_part = [=](int M) -> std::function<int()> {
             const double wD = ((double)N / M) * ((double)N / M) * ((double)N / M);
             return [=]() {
                 int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
-                // D part (FP32)
                 PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.a, sa.band, c->f.work, &Sa, &ha, 0, M));
                 if (G.a != G.b)
                     PS_TRY(c2r_xy<float>(c, LOAD_MASKED, dtable + G.b, sb.band, c->f.work2, &Sb, &hbb, 0, M));
                 PS_TRY(pair_spectrum<float>(c, c->f.work, Sa, ha, G.a != G.b ? c->f.work2 : nullptr, Sb, hbb, hout,
                                             &S, 0, M));
-                PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, dtable + go, gtable.data(), ng, gD, 0, M,
-                                       wD));
+                PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT, S, hout, dtable + go, gtable.data(), ng, sumD, 0, M,
+                                       wD, didx + io));
                 if (kappa)
-                    PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, dtable + go, gtable.data(), ng, gA,
-                                           0, M, wD));
-                // I part (FP64 counts on the xy-quadrant: unit filters are even in every axis)
+                    PS_TRY(dot_pass<float>(c, c->f.work3, SPEC_DOT_ABS, S, hout, dtable + go, gtable.data(), ng, sumA,
+                                           0, M, wD, didx + io));
+                return PS_OK;
+            };
+        };
+        auto i_part = [=](int M) -> std::function<int()> {
+            return [=]() {
+                int Sa = 0, ha = 0, Sb = 0, hbb = 0, S = 0;
                 PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.a, sa.band, c->d.work, &Sa, &ha, 1, M));
                 if (G.a != G.b)
                     PS_TRY(c2r_xy<double>(c, LOAD_UNIT, dtable + G.b, sb.band, c->d.work2, &Sb, &hbb, 1, M));
                 PS_TRY(pair_spectrum<double>(c, c->d.work, Sa, ha, G.a != G.b ? c->d.work2 : nullptr, Sb, hbb, hout,
                                              &S, 1, M));
-                PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, dtable + go, gtable.data(), ng, gI, 1,
-                                        M));
+                PS_TRY(dot_pass<double>(c, c->d.work3, SPEC_COUNT, S, hout, dtable + go, gtable.data(), ng, sumI, 1,
+                                        M, 1.0, didx + io));
                 return PS_OK;
+            };
+        };
+        auto group_op = [=](int M) -> std::function<int()> {
+            const auto dp = d_part(M), ip = i_part(M);
+            return [=]() {
+                PS_TRY(dp());
+                return ip();
             };
         };
         int M = alias_free_grid(N, ba, bb, hmax);
@@ -1477,15 +1522,27 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             PS_TRY(tables_for<float>(c, M, &t32));
             PS_TRY(tables_for<double>(c, M, &t64));
         }
-        const auto gop = group_op(M);
+        if (g == 0) {  // fork the side lane (after the DERIVED chain the counts read)
+            ops.push_back([=]() {
+                PS_CK(cudaEventRecord(c->ev_fork, c->stream));
+                PS_CK(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
+                return PS_OK;
+            });
+        }
+        const auto dop = d_part(M), iop = i_part(M);
         ops.push_back([=]() {
-            PS_TRY(gop());
-            PS_TRY(scatter_dev(c, gD, didx + io, ng, sumD));
-            PS_TRY(scatter_dev(c, gI, didx + io, ng, sumI));
-            if (kappa) PS_TRY(scatter_dev(c, gA, didx + io, ng, sumA));
-            return PS_OK;
+            PS_TRY(dop());
+            SideLane lane(c);
+            return iop();
         });
         (void)hsh;
+    }
+    if (!groups.empty()) {  // join the side lane
+        ops.push_back([=]() {
+            PS_CK(cudaEventRecord(c->ev_join, c->side_stream));
+            PS_CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+            return PS_OK;
+        });
     }
     // ---- n = 2 (Parseval): one k-space pass per chunk
     for (const P2Chunk ch : p2) {
@@ -1940,8 +1997,14 @@ int ps_gpu_create(ps_gpu_ctx** out, int nbins, double boxsize, int methods, int 
             rc = fail(PS_ERR_CUDA, "event creation failed");
             break;
         }
-        if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess) {
             rc = fail(PS_ERR_CUDA, "stream creation failed");
+            break;
+        }
+        if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "event creation failed");
             break;
         }
         bool ev_ok = true;
@@ -2392,6 +2455,14 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->side_stream) {
+        cudaStreamSynchronize(c->side_stream);
+        cudaStreamDestroy(c->side_stream);
+    }
+    cudaFree(c->side_partials);
+    cudaFree(c->side_lut);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     delete c;
 }
 

@@ -149,16 +149,22 @@ enum InvLoad : int { LOAD_PLAIN = 0, LOAD_MASKED = 1, LOAD_UNIT = 2 };
 template <typename T, int N>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     k_inv_x(const V2<T>* __restrict__ src, int src_stride, int nsrc, V2<T>* __restrict__ dst, int dst_stride,
-            int mode, const Shell* __restrict__ shell_p, int hvalid, int quad, const V2<T>* __restrict__ tw_g)
+            int mode, const Shell* __restrict__ shell_p, int hvalid, int quad, int skip_dead,
+            const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tiles_per_row = dst_stride / G::W;
+    // skip_dead: a filtered tile whose |my| exceeds the shell's band holds only
+    // zeros and is not written (the inverse Y pass then treats those rows as
+    // zero, its jband)
+    if (skip_dead && mode != LOAD_PLAIN && abs(lattice_freq((int)(blockIdx.x / tiles_per_row), N)) > shell_p->band)
+        return;
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
     __syncthreads();
     SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), (int)(threadIdx.x % G::W)};
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
-    const int tiles_per_row = dst_stride / G::W;
     // quad: pencils j <= N/2 only, outputs i <= N/2 only, stored [i][j][h] with
     // N/2+1 rows per plane (the unit filter is even in every axis).
     // nsrc: grid size of the source spectrum ([nsrc][nsrc][src_stride]); a mode
@@ -210,7 +216,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 // ------------------------------------------------------------------ Y pass
 template <typename T, int N, bool INV>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
-    k_pass_y(V2<T>* __restrict__ data, int stride, int quad, const V2<T>* __restrict__ tw_g)
+    k_pass_y(V2<T>* __restrict__ data, int stride, int quad, int jband, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
@@ -223,11 +229,14 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     const int i = blockIdx.x / tiles_per_plane;
     const int h = (blockIdx.x % tiles_per_plane) * G::W + w;
     V* base = data + (size_t)i * nj * stride + h;
+    // jband < N/2: rows with |my| > jband are zero and not read (the inverse X
+    // pass of a band-limited shell leaves them unwritten)
     V a[G::R];
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int j = t + G::TPF * e;
-        a[e] = base[(size_t)(quad && j > N / 2 ? N - j : j) * stride];
+        const int jr = quad && j > N / 2 ? N - j : j;
+        a[e] = (jband >= N / 2 || abs(lattice_freq(j, N)) <= jband) ? base[(size_t)jr * stride] : czero<V>();
     }
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
     __syncthreads();
@@ -874,15 +883,17 @@ static __global__ void k_scatter(const double* __restrict__ src, const int* __re
 
 // ------------------------------------------------------------------ final sums
 // out[c] = sum_b partials[c*nblocks + b], fixed order (one CTA per column).
+// Column c of the partial sums, summed in a fixed order, lands in
+// out[c * out_stride], or in out[idx[c]] (the configuration it belongs to).
 static __global__ void k_sum_partials(const double* __restrict__ partials, int nblocks, double* out,
-                                      int out_stride)
+                                      int out_stride, const int* __restrict__ idx)
 {
     __shared__ double red[32];
     const double* p = partials + (size_t)blockIdx.x * nblocks;
     double s = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += p[b];
     s = block_sum<1024>(s, red);
-    if (threadIdx.x == 0) out[(size_t)blockIdx.x * out_stride] = s;
+    if (threadIdx.x == 0) out[idx ? (size_t)idx[blockIdx.x] : (size_t)blockIdx.x * out_stride] = s;
 }
 
 // ------------------------------------------------------------------ DERIVED k-range

@@ -74,25 +74,29 @@ template <typename T, int N> struct L3 {
     // quad: the xy-quadrant layout of data even in x and y ([i <= N/2][j <= N/2][h])
     // nsrc: grid size of the source spectrum src (0: N; a larger field grid
     // when this N-grid holds a band-limited sub-grid transform)
+    // skip_dead: tiles of all-zero pencils (|my| above the shell's band) are
+    // left unwritten; the following pass_y must then be given that band
     static int inv_x(cudaStream_t st, const V* src, int ss, V* dst, int ds, int mode, const Shell* sh,
-                     int hvalid, const Tables<T>& tb, int quad = 0, int nsrc = 0)
+                     int hvalid, const Tables<T>& tb, int quad = 0, int nsrc = 0, int skip_dead = 0)
     {
         PS_LTRY(set_smem(k_inv_x<T, N>, PG::SMEM));
         const int nj = quad ? N / 2 + 1 : N;
         k_inv_x<T, N><<<(unsigned)(nj * (ds / PG::W)), PG::THREADS, PG::SMEM, st>>>(
-            src, ss, nsrc > 0 ? nsrc : N, dst, ds, mode, sh, hvalid, quad, tb.twp);
+            src, ss, nsrc > 0 ? nsrc : N, dst, ds, mode, sh, hvalid, quad, skip_dead, tb.twp);
         return PS_OK;
     }
-    static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb, int quad = 0)
+    // jband < N/2: input rows with |my| > jband are zero and are not read
+    static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb, int quad = 0,
+                      int jband = N)
     {
         const int ni = quad ? N / 2 + 1 : N;
         const unsigned blocks = (unsigned)(ni * (stride / PG::W));
         if (inv) {
             PS_LTRY(set_smem(k_pass_y<T, N, true>, PG::SMEM));
-            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, tb.twp);
+            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, jband, tb.twp);
         } else {
             PS_LTRY(set_smem(k_pass_y<T, N, false>, PG::SMEM));
-            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, tb.twp);
+            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, jband, tb.twp);
         }
         return PS_OK;
     }

@@ -143,11 +143,11 @@ int run_noalloc(cudaStream_t st, unsigned char* base, double L, const float* fie
         PS_LTRY((L3<float, N>::inv_x(st, spec32, S32, work32, Sd, LOAD_MASKED, shells + s, N / 2 + 1, tb32)));
         PS_LTRY((L3<float, N>::pass_y(st, work32, Sd, true, tb32)));
         PS_LTRY((L3<float, N>::inv_z(st, work32, Sd, hb, nullptr, nullptr, EPI_REDUCE, 2, partials, tb32, &nb)));
-        k_sum_partials<<<1, 1024, 0, st>>>(partials, nb, sums + s, 1);
+        k_sum_partials<<<1, 1024, 0, st>>>(partials, nb, sums + s, 1, nullptr);
         PS_LTRY((L3<double, N>::inv_x(st, nullptr, S64, work64, Si, LOAD_UNIT, shells + s, N / 2 + 1, tb64)));
         PS_LTRY((L3<double, N>::pass_y(st, work64, Si, true, tb64)));
         PS_LTRY((L3<double, N>::inv_z(st, work64, Si, hb, nullptr, nullptr, EPI_REDUCE, 2, partials, tb64, &nb)));
-        k_sum_partials<<<1, 1024, 0, st>>>(partials, nb, sums + ns + s, 1);
+        k_sum_partials<<<1, 1024, 0, st>>>(partials, nb, sums + ns + s, 1, nullptr);
     }
     const double n3 = (double)N * (double)N * (double)N;
     k_noalloc_finalize<<<(ns + 127) / 128, 128, 0, st>>>(ns, host_norm_coef(L, N, 2), n3, sums, out);
