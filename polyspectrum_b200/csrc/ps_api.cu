@@ -335,12 +335,16 @@ int ensure_lut(ps_gpu_ctx* c, size_t n)
 }
 // While alive, the context's stream, partial sums and shell table are those
 // of the side lane (every launch helper then works on the side lane).
+// With per-kernel profiling on, everything stays on the main lane, so the
+// events around each launch time that launch alone.
 struct SideLane {
     ps_gpu_ctx* c;
-    explicit SideLane(ps_gpu_ctx* cc) : c(cc) { swap(); }
+    bool on;
+    explicit SideLane(ps_gpu_ctx* cc, bool always = false) : c(cc), on(always || !cc->prof_on) { swap(); }
     ~SideLane() { swap(); }
     void swap()
     {
+        if (!on) return;
         std::swap(c->stream, c->side_stream);
         std::swap(c->partials, c->side_partials);
         std::swap(c->partials_cap, c->side_partials_cap);
@@ -1405,7 +1409,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         PS_TRY(ensure_partials(c, np));
         PS_TRY(ensure_lut(c, (size_t)3 * (N / 2) * (N / 2) + 2));
         if (!groups.empty()) {
-            SideLane lane(c);
+            SideLane lane(c, true);  // the side lane's own scratch, profiling or not
             PS_TRY(ensure_partials(c, np));
             PS_TRY(ensure_lut(c, (size_t)3 * (N / 2) * (N / 2) + 2));
         }

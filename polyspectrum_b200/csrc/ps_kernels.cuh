@@ -55,7 +55,9 @@ template <typename T, int N> struct PencilGeom {
 // which use radix 8 and 64 threads (two transforms must fit in registers).
 template <typename T, int NH> struct RowRadix {
     static constexpr bool POW2 = (NH & (NH - 1)) == 0;
-    static constexpr int value = !POW2 ? DefaultRadix<NH>::value
+    // rows of 160 (320-point grids): radix 10 keeps two row transforms in
+    // registers (radix 20 needed over 220 registers per thread)
+    static constexpr int value = NH == 160 ? 10 : !POW2 ? DefaultRadix<NH>::value
                                : NH <= 16 ? NH : ((sizeof(T) == 4 && NH == 512) ? 16 : 8);
 };
 template <typename T, int N> struct RowGeom {
