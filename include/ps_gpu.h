@@ -202,6 +202,16 @@ int ps_gpu_grad(ps_gpu_ctx *ctx, int method, int n, const double *k, const doubl
                 const double *kmax, double kbinwidth, int kbinningCase, void *out,
                 int out_is_double, int out_mem);
 
+/* Band-limited field spectrum: later loads (ps_gpu_set_field*) compute only
+ * the modes whose three |components| are at most `band` (band < 0 or >= N/2:
+ * all modes, the default).  Modes outside are left undefined, and every
+ * computation that would read one returns PS_ERR_ARG, so results are the same
+ * as with the full spectrum.  A plan's band (ps_gpu_plan_band: the largest
+ * |component| of a mode any of its shells holds) is the narrowest band that
+ * serves it.  No reference counterpart (the reference transforms all modes). */
+int ps_gpu_set_spectrum_band(ps_gpu_ctx *ctx, int band);
+int ps_gpu_plan_band(const ps_gpu_plan *plan);
+
 /* With on != 0, later phase-only loads (use_only_phase = 1) also keep |X| per
  * mode of the field spectrum (one more real half-spectrum on the device), which
  * ps_gpu_grad needs to differentiate through z/|z| (utils_fftw.c:78-93).  No

@@ -90,6 +90,8 @@ def lib() -> C.CDLL:
     L.ps_gpu_launch_count.restype = C.c_longlong
     L.ps_gpu_tune_export.argtypes = [vp, C.c_char_p, ip]
     L.ps_gpu_keep_modulus.argtypes = [vp, ip]
+    L.ps_gpu_set_spectrum_band.argtypes = [vp, ip]
+    L.ps_gpu_plan_band.argtypes = [vp]
     L.ps_gpu_tune_import.argtypes = [vp, C.c_char_p]
     L.ps_gpu_set_profiling.argtypes = [vp, ip]
     L.ps_gpu_kernel_stats.argtypes = [vp, C.POINTER(ps_kernel_stat), ip]
@@ -104,7 +106,8 @@ def lib() -> C.CDLL:
                  "ps_gpu_set_stream", "ps_gpu_last_timing", "ps_gpu_set_profiling",
                  "ps_gpu_kernel_stats", "ps_gpu_plan_create", "ps_gpu_plan_execute",
                  "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize",
-                 "ps_gpu_tune_export", "ps_gpu_tune_import", "ps_gpu_keep_modulus"):
+                 "ps_gpu_tune_export", "ps_gpu_tune_import", "ps_gpu_keep_modulus",
+                 "ps_gpu_set_spectrum_band", "ps_gpu_plan_band"):
         getattr(L, name).restype = ip
     _lib = L
     return L
@@ -268,6 +271,10 @@ class Context:
         """A reusable plan of these configurations (ps_gpu_plan_create)."""
         return Plan(self, cfgs, method, graph, kappa, autotune)
 
+    def set_spectrum_band(self, band: int):
+        """Later loads compute only modes with |components| <= band (-1: all)."""
+        _check(lib().ps_gpu_set_spectrum_band(self._h, int(band)))
+
     def keep_modulus(self, on: bool = True):
         """Phase-only loads keep |X| so grad() can differentiate through z/|z|."""
         _check(lib().ps_gpu_keep_modulus(self._h, int(bool(on))))
@@ -342,6 +349,11 @@ class Plan:
         _check(lib().ps_gpu_plan_execute(self.ctx.handle, self._h, _dptr(B), _dptr(Np),
                                          _dptr(kap) if self.kappa else None, out))
         return B, Np, kap, out
+
+    @property
+    def band(self) -> int:
+        """Largest |component| of a mode this plan reads (ps_gpu_plan_band)."""
+        return _check(lib().ps_gpu_plan_band(self._h))
 
     def submit(self) -> "Submission":
         """Queue one execution on the field most recently loaded (ps_gpu_plan_submit);

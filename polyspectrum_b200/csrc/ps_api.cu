@@ -142,6 +142,10 @@ struct ps_gpu_ctx {
     long long launches_total = 0;  // kernels executed since creation (graph replays included)
     int use_only_phase = 0;
     bool keep_modulus = false;  // phase-only loads keep |X| (phase-only adjoint)
+    // field spectrum band: loads compute only modes whose |components| are at
+    // most spec_band (-1: all); loaded_band is that of the field loaded last
+    int spec_band = -1;
+    int loaded_band = 0;
     bool field_set = false;
     // per-kernel profiling (ps_gpu_set_profiling)
     struct ProfRec {
@@ -578,25 +582,32 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
         PS_TRY(alloc_dev(&B.mod, (size_t)N * N * B.S));
         mod = B.mod;
     }
-    const double V = sizeof(V2<T>), NN2 = (double)N * N, H = N / 2 + 1;
+    // band-limited spectrum: columns h <= band, rows and outputs |m| <= band
+    const int band = (c->spec_band >= 0 && c->spec_band < N / 2) ? c->spec_band : N / 2;
+    const int hcols = band + 1;
+    const int ncols = std::min(B.S, round_up(hcols, pw<T>(N)));
+    const double V = sizeof(V2<T>), NN2 = (double)N * N, H = hcols;
     const double src_bytes = kind == SRC_F32 ? 4.0 : kind == SRC_F64 ? 8.0 : kind == SRC_XHI_F32 ? 8.0 : 16.0;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, N / 2 + 1, B.tables()))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, hcols, B.tables()))));
         pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * H * V, N);
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tables()))));
-        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * B.S * V, N);
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tables(), 0, NN, ncols))));
+        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * ncols * V, N);
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.spec, B.S, N / 2 + 1, epi, B.spec, B.S, nullptr, 0,
+        const double rows = band < N / 2 ? (double)N * (2 * band + 1) : NN2;
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, B.spec, B.S, hcols, epi, B.spec, B.S, nullptr, 0,
                                                 nullptr, 0, nullptr, 0, nullptr, B.tables(), nullptr, 1.0, 0, 0,
-                                                0x7fffffff, mod))));
-        pf.end(fam<T>(KF_FWD_X_STORE), 2.0 * NN2 * H * V, N);
+                                                0x7fffffff, mod, ncols, band < N / 2 ? band : NN))));
+        pf.end(fam<T>(KF_FWD_X_STORE), rows * H * V + (band < N / 2 ? (double)(2 * band + 1) : (double)N) *
+                                                         (2 * band + 1 < N ? 2 * band + 1 : N) * H * V, N);
     }
+    c->loaded_band = band;
     PS_CK(cudaGetLastError());
     B.have_spec = true;
     B.have_mod = mod != nullptr;
@@ -867,6 +878,22 @@ double norm_coef(double L, int N, int n)
 // =========================================================================
 // method 1: plain FP64, reference dataflow
 // =========================================================================
+// A computation reaching modes of band `need` on a field loaded with a
+// narrower spectrum band (ps_gpu_set_spectrum_band) is refused.
+int check_band(const ps_gpu_ctx* c, int need)
+{
+    if (need > c->loaded_band)
+        return fail(PS_ERR_ARG, "the field was loaded with spectrum band %d; this computation reaches modes of band %d",
+                    c->loaded_band, need);
+    return PS_OK;
+}
+int legs_band(const std::vector<Shell>& legs, int N)
+{
+    int b = 0;
+    for (const Shell& sh : legs) b = std::max(b, std::min(sh.band, N / 2));
+    return b;
+}
+
 int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, double* kappa)
 {
     if (!c->d.have_spec) return fail(PS_ERR_ARG, "FP64 spectrum not available (methods mask)");
@@ -877,6 +904,7 @@ int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, d
     std::vector<double> coef(nconf), habs(nconf, 0.0);
     for (int q = 0; q < nconf; q++) {
         PS_TRY(resolve_legs(c, 1, cfgs + q, legs));
+        PS_TRY(check_band(c, legs_band(legs[0], N)));
         const int n = cfgs[q].n;
         PS_CK(cudaMemcpyAsync(c->dshells, legs[0].data(), sizeof(Shell) * n, cudaMemcpyHostToDevice,
                               c->stream));
@@ -1048,6 +1076,7 @@ struct ps_gpu_plan {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     long long graph_launches = 0;  // kernels in the captured graph
+    int band = 0;                  // largest |component| of a mode the plan reads
 };
 
 namespace {
@@ -1305,6 +1334,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
     // ---- shell table: [unique shells][group closing lists][n=2 chunk tables]
     std::vector<Shell> table(nu);
     for (int u = 0; u < nu; u++) table[u] = host_shell_of(u);
+    P->band = legs_band(table, N);
     std::vector<int> gofs(groups.size()), copy_src, copy_dst;
     for (size_t g = 0; g < groups.size(); g++) {
         gofs[g] = (int)table.size();
@@ -1762,6 +1792,7 @@ int batched(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, doubl
     P->flags = kappa ? PS_PLAN_KAPPA : 0;
     P->cfgs.assign(cfgs, cfgs + nconf);
     int rc = plan_batched(c, P);
+    if (rc == PS_OK) rc = check_band(c, P->band);
     if (rc == PS_OK) rc = plan_enqueue(c, P);
     if (rc == PS_OK) rc = plan_finish(c, P, B, Np, kappa, cfgs);
     plan_free(P);
@@ -2146,6 +2177,7 @@ int ps_gpu_grad(ps_gpu_ctx* c, int method, int n, const double* k, const double*
     PS_TRY(timed_begin(c));
     std::vector<std::vector<Shell>> legs;
     PS_TRY(resolve_legs(c, 1, &g, legs));
+    PS_TRY(check_band(c, legs_band(legs[0], c->N)));
     const double n3 = (double)c->N * (double)c->N * (double)c->N;
     const double scale = norm_coef(c->L, c->N, n) / (Np * n3);
     int rc = method == PS_FP64_PLAIN ? grad_impl<double>(c, n, legs[0], scale, out, out_is_double, out_mem)
@@ -2290,6 +2322,7 @@ int ps_gpu_plan_execute(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly,
             for (int q = 0; q < P->nconf; q++) cfgs_out[q] = g[q];
     } else {
         if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available");
+        PS_TRY(check_band(c, P->band));
         if ((P->flags & PS_PLAN_GRAPH) && c->prof_on) PS_TRY(plan_enqueue(c, P));  // profiled: eager
         else PS_TRY(plan_run(c, P));
         PS_TRY(plan_finish(c, P, B, Npoly, kappa, cfgs_out));
@@ -2319,6 +2352,7 @@ int ps_gpu_plan_submit(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly, 
     if (kappa && !(P->flags & PS_PLAN_KAPPA)) return fail(PS_ERR_ARG, "plan created without PS_PLAN_KAPPA");
     if (P->nconf == 0) return PS_OK;
     if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available");
+    PS_TRY(check_band(c, P->band));
     PS_CK(cudaSetDevice(c->device));
     if ((P->flags & PS_PLAN_GRAPH) && c->prof_on) PS_TRY(plan_enqueue(c, P));
     else PS_TRY(plan_run(c, P));
@@ -2345,6 +2379,22 @@ int ps_gpu_synchronize(ps_gpu_ctx* c)
 }
 
 long long ps_gpu_launch_count(ps_gpu_ctx* c) { return c ? c->launches_total : -1; }
+
+int ps_gpu_set_spectrum_band(ps_gpu_ctx* c, int band)
+{
+    g_err[0] = 0;
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    c->spec_band = band;
+    return PS_OK;
+}
+
+int ps_gpu_plan_band(const ps_gpu_plan* P)
+{
+    g_err[0] = 0;
+    if (!P) return fail(PS_ERR_ARG, "plan is NULL");
+    if (P->method != PS_FP32_BATCHED) return P->ctx ? P->ctx->N / 2 : 0;
+    return P->band;
+}
 
 int ps_gpu_keep_modulus(ps_gpu_ctx* c, int on)
 {

@@ -218,13 +218,13 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 // ------------------------------------------------------------------ Y pass
 template <typename T, int N, bool INV>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
-    k_pass_y(V2<T>* __restrict__ data, int stride, int quad, int jband, const V2<T>* __restrict__ tw_g)
+    k_pass_y(V2<T>* __restrict__ data, int stride, int ncols, int quad, int jband, const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
-    const int tiles_per_plane = stride / G::W;
+    const int tiles_per_plane = ncols / G::W;  // columns h < ncols of rows of stride `stride`
     // quad: planes i <= N/2, rows j <= N/2 stored, row N-j read as row j
     // (data even in y)
     const int nj = quad ? N / 2 + 1 : N;
@@ -582,13 +582,17 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, int ndk, const Shell* __restrict__ shells,
             int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight, int quad,
-            int r2max, double* __restrict__ partials, const V2<T>* __restrict__ tw_g, T* __restrict__ mod_out)
+            int r2max, double* __restrict__ partials, const V2<T>* __restrict__ tw_g, T* __restrict__ mod_out,
+            int ncols, int jband)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;
-    const int tiles_per_row = stride / G::W;
+    // pencils of columns h < ncols (rows of stride `stride`); storing passes
+    // with jband < N/2 (a band-limited field spectrum) skip the tiles whose
+    // |my| exceeds it and write only modes with |mx| <= jband
+    const int tiles_per_row = ncols / G::W;
     // quad (counts only): pencils j <= N/2 of data even in x and y stored
     // [i <= N/2][j <= N/2][h]; plane N-i read as plane i; interior j weigh 2
     const int nj = quad ? N / 2 + 1 : N;
@@ -597,6 +601,9 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
     const bool col_ok = h < hvalid && h <= N / 2;
     const int my = lattice_freq(j, N);
     const int mz = h == N / 2 ? -(N / 2) : h;
+    if constexpr (!DOT) {
+        if (jband < N / 2 && abs(my) > jband) return;  // rows outside the field's band
+    }
     if constexpr (DOT) {
         // the whole tile outside every shell: no transform, zero partials
         const bool live = col_ok && my * my + mz * mz <= r2max;
@@ -653,6 +660,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
 #pragma unroll
         for (int e = 0; e < G::R; e++) {
             const int i = t + G::TPF * e;
+            if (jband < N / 2 && abs(lattice_freq(i, N)) > jband) continue;
             V v = a[e];
             if (epi == SPEC_STORE_PHASE) {
                 // mod_out (optional) keeps |X| for the phase-only adjoint

@@ -86,17 +86,19 @@ template <typename T, int N> struct L3 {
         return PS_OK;
     }
     // jband < N/2: input rows with |my| > jband are zero and are not read
+    // ncols (0: stride): only columns h < ncols, a multiple of the pencil width
     static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb, int quad = 0,
-                      int jband = N)
+                      int jband = N, int ncols = 0)
     {
         const int ni = quad ? N / 2 + 1 : N;
-        const unsigned blocks = (unsigned)(ni * (stride / PG::W));
+        const int nc = ncols > 0 ? ncols : stride;
+        const unsigned blocks = (unsigned)(ni * (nc / PG::W));
         if (inv) {
             PS_LTRY(set_smem(k_pass_y<T, N, true>, PG::SMEM));
-            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, jband, tb.twp);
+            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, nc, quad, jband, tb.twp);
         } else {
             PS_LTRY(set_smem(k_pass_y<T, N, false>, PG::SMEM));
-            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, quad, jband, tb.twp);
+            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, nc, quad, jband, tb.twp);
         }
         return PS_OK;
     }
@@ -141,21 +143,23 @@ template <typename T, int N> struct L3 {
     static int fwd_x(cudaStream_t st, V* data, int stride, int hvalid, int epi, V* out, int ostride,
                      const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
                      int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0,
-                     int quad = 0, int ndk = 0, int r2max = 0x7fffffff, T* mod_out = nullptr)
+                     int quad = 0, int ndk = 0, int r2max = 0x7fffffff, T* mod_out = nullptr, int ncols = 0,
+                     int jband = N)
     {
         const int nj = quad ? N / 2 + 1 : N;
-        const unsigned blocks = (unsigned)(nj * (stride / PG::W));
+        const int nc = ncols > 0 ? ncols : stride;
+        const unsigned blocks = (unsigned)(nj * (nc / PG::W));
         const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT || epi == SPEC_DOT_ABS;
         if (dot) {
             PS_LTRY(set_smem(k_fwd_x<T, N, true>, PG::SMEM));
             k_fwd_x<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(
                 data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
-                weight, quad, r2max, partials, tb.twp, mod_out);
+                weight, quad, r2max, partials, tb.twp, mod_out, nc, jband);
         } else {
             PS_LTRY(set_smem(k_fwd_x<T, N, false>, PG::SMEM));
             k_fwd_x<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(
                 data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
-                weight, quad, r2max, partials, tb.twp, mod_out);
+                weight, quad, r2max, partials, tb.twp, mod_out, nc, jband);
         }
         if (nblocks) *nblocks = (int)blocks;
         return PS_OK;

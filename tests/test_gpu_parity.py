@@ -386,3 +386,37 @@ def test_higher_polygons_match_oracle(gpu_lib, ora, legs):
     assert abs(N64[0] - n_ref) <= 1e-7 * max(1.0, n_ref)
     assert abs(B32[0] - b_ref) <= 1e-5 * abs(b_ref)
     assert N32[0] == np.rint(n_ref)
+
+
+def test_band_limited_spectrum(gpu_lib):
+    """A field loaded with a plan's spectrum band gives that plan bit-identical
+    results; computations reaching modes beyond the band are refused; a full
+    load afterwards serves them again."""
+    ps = gpu_lib
+    n_grid, box = 64, 300.0
+    dens, xhii = fields(n_grid, box)
+    dd, xx = field_args(2, dens, xhii)
+    cfgs = []
+    for k1, k2 in ((0.06, 0.09), (0.05, 0.12)):
+        c, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1, k2=k2, num_values=6, kbinningCase=1)
+        cfgs += [c[i] for i in range(len(c))]
+    p2, _, _ = ps.read_params_to_kvectors(n_grid, box, 2, num_values=2)
+    with ps.Context(n_grid, box) as ctx:
+        plan = ctx.plan(cfgs)
+        band = plan.band
+        assert 0 < band < n_grid // 2
+        ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+        full = plan.execute()
+        ctx.set_spectrum_band(band)
+        ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+        lim = plan.execute()
+        np.testing.assert_array_equal(lim[0], full[0])
+        np.testing.assert_array_equal(lim[1], full[1])
+        with pytest.raises(ps.PsError):  # all n = 2 shells reach the Nyquist band
+            ctx.batch(p2, ps.PS_FP32_BATCHED)
+        with pytest.raises(ps.PsError):
+            ctx.batch([p2[len(p2) - 1]], ps.PS_FP64_PLAIN)
+        ctx.set_spectrum_band(-1)
+        ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+        ctx.batch(p2, ps.PS_FP32_BATCHED)
+        plan.close()
