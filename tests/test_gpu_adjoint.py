@@ -120,7 +120,7 @@ def test_torch_autograd_binding(gpu_lib):
     np.testing.assert_allclose(f.grad.cpu().numpy(), 2.0 * g, rtol=0, atol=1e-12 * np.abs(g).max())
 
 
-def test_grad_config4_256(gpu_lib):
+def test_grad_equilateral_256(gpu_lib):
     """The 256^3 gradient configuration: DENS (P ~ k^-2), equilateral k = 0.8 h/Mpc, kbinwidth 1,
     DEFAULT binning; central differences (eps 1e-3, FP64) on 64 seeded voxels and 8 random
     directions; FP32 gradient against FP64."""
