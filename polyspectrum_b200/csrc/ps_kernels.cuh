@@ -467,8 +467,11 @@ __device__ __forceinline__ V2<T> load_pair(int kind, const unsigned char* ra, co
 
 // One tile per CTA (the input rows are dense and all loads are issued up front;
 // `vec`: the sources are aligned for one vector load per value pair).
+// FP32 rows of 512: at most 32 registers (no spill), so eight 256-thread CTAs
+// (every warp slot of the SM) keep their loads in flight; the pass is bound by
+// load latency.
 template <typename T, int N>
-__global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
+__global__ void __launch_bounds__(RowGeom<T, N>::THREADS, (sizeof(T) == 4 && N == 512) ? 8 : 1)
     k_fwd_z(int kind, const void* __restrict__ a_src, const void* __restrict__ b_src,
             V2<T>* __restrict__ dst, int dst_stride, int hout, int vec, const V2<T>* __restrict__ twr_g,
             const V2<T>* __restrict__ twpp_g)
