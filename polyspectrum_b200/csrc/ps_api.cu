@@ -1410,13 +1410,11 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
     double* dcoef = nullptr;
     PS_TRY(plan_upload(P, &dcoef, coef));
     const size_t gs = std::max<size_t>(nconf, 2 * MAX_DOT_SHELLS);
-    double *sumD = nullptr, *sumI = nullptr, *sumA = nullptr, *gD = nullptr, *gI = nullptr, *gA = nullptr;
+    double *sumD = nullptr, *sumI = nullptr, *sumA = nullptr, *gD = nullptr;  // gD: n = 2 chunk sums
     PS_TRY(plan_alloc(P, &sumD, nconf));
     PS_TRY(plan_alloc(P, &sumI, nconf));
     PS_TRY(plan_alloc(P, &sumA, nconf));
     PS_TRY(plan_alloc(P, &gD, gs));
-    PS_TRY(plan_alloc(P, &gI, gs));
-    PS_TRY(plan_alloc(P, &gA, gs));
     PS_TRY(plan_alloc(P, &P->dres, 2 * (size_t)nconf));
     PS_TRY(plan_alloc(P, &P->dwb, 6 * (size_t)nconf));
     PS_TRY(plan_alloc(P, &P->derr, 1));
