@@ -180,6 +180,15 @@ int ps_gpu_plan_submit(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Np
                        double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
 int ps_gpu_synchronize(ps_gpu_ctx *ctx);
 
+/* A PS_FP32_BATCHED plan execution queued on the context's stream with its
+ * results left on the device (no copy, no host callback); ps_gpu_plan_results
+ * waits for the stream and returns the results of the plan's latest
+ * execution, as ps_gpu_plan_execute does.  For loops whose per-field results
+ * are not needed on the host every time.  No reference counterpart. */
+int ps_gpu_plan_launch(ps_gpu_ctx *ctx, ps_gpu_plan *plan);
+int ps_gpu_plan_results(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
+                        double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
+
 /* The context's autotuned choices as text, one "grid N b_a b_b b_c M" line per
  * pair-group signature: writes at most buflen bytes (NUL-terminated) and
  * returns the length of the whole text, or a negative status.  Import adds

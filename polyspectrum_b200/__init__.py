@@ -91,6 +91,8 @@ def lib() -> C.CDLL:
     L.ps_gpu_tune_export.argtypes = [vp, C.c_char_p, ip]
     L.ps_gpu_keep_modulus.argtypes = [vp, ip]
     L.ps_gpu_set_spectrum_band.argtypes = [vp, ip]
+    L.ps_gpu_plan_launch.argtypes = [vp, vp]
+    L.ps_gpu_plan_results.argtypes = [vp, vp, dp, dp, dp, C.POINTER(ps_cfg)]
     L.ps_gpu_plan_band.argtypes = [vp]
     L.ps_gpu_tune_import.argtypes = [vp, C.c_char_p]
     L.ps_gpu_set_profiling.argtypes = [vp, ip]
@@ -107,7 +109,7 @@ def lib() -> C.CDLL:
                  "ps_gpu_kernel_stats", "ps_gpu_plan_create", "ps_gpu_plan_execute",
                  "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize",
                  "ps_gpu_tune_export", "ps_gpu_tune_import", "ps_gpu_keep_modulus",
-                 "ps_gpu_set_spectrum_band", "ps_gpu_plan_band"):
+                 "ps_gpu_set_spectrum_band", "ps_gpu_plan_band", "ps_gpu_plan_launch", "ps_gpu_plan_results"):
         getattr(L, name).restype = ip
     _lib = L
     return L
@@ -354,6 +356,20 @@ class Plan:
     def band(self) -> int:
         """Largest |component| of a mode this plan reads (ps_gpu_plan_band)."""
         return _check(lib().ps_gpu_plan_band(self._h))
+
+    def launch(self):
+        """Queue one execution, results left on the device (ps_gpu_plan_launch)."""
+        _check(lib().ps_gpu_plan_launch(self.ctx.handle, self._h))
+
+    def results(self):
+        """Results of the latest execution (waits): (B, Npoly, kappa, cfgs_out)."""
+        B = np.zeros(self.n)
+        Np = np.zeros(self.n)
+        kap = np.full(self.n, np.nan)
+        out = (ps_cfg * max(self.n, 1))()
+        _check(lib().ps_gpu_plan_results(self.ctx.handle, self._h, _dptr(B), _dptr(Np),
+                                         _dptr(kap) if self.kappa else None, out))
+        return B, Np, kap, out
 
     def submit(self) -> "Submission":
         """Queue one execution on the field most recently loaded (ps_gpu_plan_submit);

@@ -2364,6 +2364,34 @@ int ps_gpu_plan_submit(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly, 
     return PS_OK;
 }
 
+int ps_gpu_plan_launch(ps_gpu_ctx* c, ps_gpu_plan* P)
+{
+    g_err[0] = 0;
+    if (!c || !P) return fail(PS_ERR_ARG, "NULL argument");
+    if (P->ctx != c) return fail(PS_ERR_ARG, "plan belongs to another context");
+    if (P->method != PS_FP32_BATCHED)
+        return fail(PS_ERR_UNSUPPORTED, "launching without read-back needs a PS_FP32_BATCHED plan");
+    if (!c->field_set) return fail(PS_ERR_ARG, "no field loaded (ps_gpu_set_field)");
+    if (P->nconf == 0) return PS_OK;
+    if (!c->f.have_spec) return fail(PS_ERR_ARG, "FP32 spectrum not available");
+    PS_TRY(check_band(c, P->band));
+    PS_CK(cudaSetDevice(c->device));
+    if ((P->flags & PS_PLAN_GRAPH) && c->prof_on) return plan_enqueue(c, P);
+    return plan_run(c, P);
+}
+
+int ps_gpu_plan_results(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly, double* kappa, ps_cfg* cfgs_out)
+{
+    g_err[0] = 0;
+    if (!c || !P || !B || !Npoly) return fail(PS_ERR_ARG, "NULL argument");
+    if (P->ctx != c) return fail(PS_ERR_ARG, "plan belongs to another context");
+    if (P->method != PS_FP32_BATCHED) return fail(PS_ERR_UNSUPPORTED, "results of a PS_FP32_BATCHED plan only");
+    if (kappa && !(P->flags & PS_PLAN_KAPPA)) return fail(PS_ERR_ARG, "plan created without PS_PLAN_KAPPA");
+    if (P->nconf == 0) return PS_OK;
+    PS_CK(cudaSetDevice(c->device));
+    return plan_finish(c, P, B, Npoly, kappa, cfgs_out);
+}
+
 int ps_gpu_synchronize(ps_gpu_ctx* c)
 {
     g_err[0] = 0;

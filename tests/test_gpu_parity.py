@@ -420,3 +420,28 @@ def test_band_limited_spectrum(gpu_lib):
         ctx.get_FT_field(2, dd, xx, use_only_phase=1)
         ctx.batch(p2, ps.PS_FP32_BATCHED)
         plan.close()
+
+
+def test_plan_launch_and_results(gpu_lib):
+    """Executions queued without read-back (ps_gpu_plan_launch) over several
+    fields; ps_gpu_plan_results returns exactly the latest execution's
+    results, DERIVED write-back included."""
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    cfgs, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=0.1, k2=0.14, num_values=5, kbinningCase=1)
+    f1 = field_args(2, *fields(n_grid, box))
+    f2 = field_args(2, *fields(n_grid, box, seed=7))
+    with ps.Context(n_grid, box) as ctx:
+        plan = ctx.plan(cfgs)
+        ctx.get_FT_field(2, *f2, use_only_phase=1)
+        want = plan.execute()
+        for f in (f1, f2, f1, f2):
+            ctx.set_field_async(2, *f, use_only_phase=1)
+            plan.launch()
+        B, Np, _, out = plan.results()
+        ctx.synchronize()
+        plan.close()
+    np.testing.assert_array_equal(B, want[0])
+    np.testing.assert_array_equal(Np, want[1])
+    for i in range(len(cfgs)):
+        assert list(out[i].kmin)[:3] == list(want[3][i].kmin)[:3]
