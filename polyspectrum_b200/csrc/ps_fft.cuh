@@ -3,8 +3,9 @@
 // A transform of length N is done by TPF = N/R threads.  Thread t holds
 // a[e] = x[t + TPF*e] ("canonical layout") on entry and X[t + TPF*e] on exit.
 // N is a power of two, or 3 or 5 times one (sub-grid transforms).  Passes are
-// radix-R (for N = f 2^k, R = f 2^r: one radix-R pass, then radix 2^r), the
-// last one possibly of a smaller radix; each thread then does R/Rp butterflies.  Pass p with radix Rp and span Ns (product of the
+// radix-R (for N = f 2^k, R = f 2^r: radix-2^r passes, one of a smaller power
+// of two if needed, then one radix-R pass last); each thread does R/Rp
+// butterflies per pass.  Pass p with radix Rp and span Ns (product of the
 // previous radices) computes, for butterfly v in [0, N/Rp):
 //     b_q = x[v + q*N/Rp] * W_{Ns*Rp}^{q*(v mod Ns)},  b = DFT_Rp(b),
 //     y[(v/Ns)*Ns*Rp + (v mod Ns) + q*Ns] = b_q
@@ -161,24 +162,27 @@ template <bool INV> struct Dft<5, INV> {
     }
 };
 
-// Radix plan.  R = f 2^r with f in {1, 3, 5} the odd part of N: for f = 1,
-// passes of radix R while possible, then one pass of the remainder; for f > 1
-// one pass of radix R first (it carries the odd factor), then the same scheme
-// with radix 2^r on N / R.  Every radix divides R.
+// Radix plan.  R = f 2^r with f in {1, 3, 5} the odd part of N: passes of
+// radix 2^r while possible, then one pass of the power-of-two remainder; for
+// f > 1 these cover N / R and one radix-R pass (it carries the odd factor)
+// comes last.  Every radix divides R.  With the odd pass last, every pass
+// that goes through shared memory has a power-of-two radix and span, which
+// the row layout (SmemRow) makes conflict-free.
 template <int N, int R> struct RadixPlan {
     __host__ __device__ static constexpr int odd_of(int n) { return n % 2 ? n : odd_of(n / 2); }
     static constexpr int F = odd_of(R);
     static constexpr int R2 = R / F;                  // radix of the power-of-two passes
-    static constexpr int HEAD = F > 1 ? 1 : 0;        // the radix-R pass of a mixed length
+    static constexpr int TAIL = F > 1 ? 1 : 0;        // the radix-R pass of a mixed length
     static constexpr int N2 = N / (F > 1 ? R : 1);    // what the power-of-two passes cover
     __host__ __device__ static constexpr int count_full(int n) { return n >= R2 ? 1 + count_full(n / R2) : 0; }
     __host__ __device__ static constexpr int rem_of(int n) { return n >= R2 ? rem_of(n / R2) : n; }
     static constexpr int FULL = count_full(N2);
     static constexpr int REM = rem_of(N2);  // 1 if N2 is a power of R2
-    static constexpr int P = HEAD + FULL + (REM > 1 ? 1 : 0);
+    static constexpr int NREM = REM > 1 ? 1 : 0;
+    static constexpr int P = FULL + NREM + TAIL;
     __host__ __device__ static constexpr int radix(int p)
     {
-        return p < HEAD ? R : (p < HEAD + FULL ? R2 : REM);
+        return p < FULL ? R2 : (p < FULL + NREM ? REM : R);
     }
     __host__ __device__ static constexpr int span(int p)
     {
@@ -261,13 +265,13 @@ __device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* _
             } else {
                 const int j = (v / Ns) * Ns * Rp + k;
 #pragma unroll
-                for (int q = 0; q < Rp; q++) sm.st(j + q * Ns, b[q]);
+                for (int q = 0; q < Rp; q++) sm.template st<Rp, Ns>(j + q * Ns, b[q]);
             }
         }
         if constexpr (!LAST) {
             sync();
 #pragma unroll
-            for (int e = 0; e < R; e++) a[e] = sm.ld(t + TPF * e);
+            for (int e = 0; e < R; e++) a[e] = sm.template ld<Rp, Ns>(t + TPF * e);
             sync();
             fft_passes<V, N, R, INV, P_ + 1>(a, t, sm, twt, sync);
         }
@@ -298,20 +302,40 @@ template <typename V, int N, int R> inline void stockham_table(V* out)
 template <typename V, int W> struct SmemInterleaved {
     V* s;
     int lane;
-    __device__ __forceinline__ void st(int pos, V v) { s[pos * W + lane] = v; }
-    __device__ __forceinline__ V ld(int pos) const { return s[pos * W + lane]; }
+    template <int Rp, int Ns> __device__ __forceinline__ void st(int pos, V v) { s[pos * W + lane] = v; }
+    template <int Rp, int Ns> __device__ __forceinline__ V ld(int pos) const { return s[pos * W + lane]; }
 };
 
 // Shared-memory accessor for row passes: one row per transform, XOR-swizzled
-// within 128-byte groups: element pos lives at pos ^ ((pos >> LB) & (G-1)),
-// G = 2^LB elements per 128 bytes.  Stockham writes of stride Rp (and 2, 4
-// interleaved runs) then hit G distinct bank groups per 128-byte wavefront,
-// and reads of consecutive positions stay conflict-free.
+// within blocks of G = 2^LB elements (128 bytes): element pos of block
+// a = pos >> LB lives at pos ^ g(a).
+//  * Exchange after a pass of radix Rp and span Ns (both powers of two): the
+//    stores of one instruction put lane t at (t/Ns)*Ns*Rp + t%Ns + q*Ns.
+//    When Ns*Rp < G the lanes that share an offset within their block differ
+//    in a mod Rp, and g(a) = a*Ns moves them apart on the log2(Rp) bits that
+//    q occupies; when Ns*Rp >= G they differ in a / K (K = Ns*Rp/G) and
+//    g(a) = (a/K)*Ns does the same.  The loads that follow (consecutive
+//    positions, one block per G lanes) stay conflict-free under any g.
+//  * Elsewhere (r2c post-processing): g(a) = a.
 template <typename V> struct SmemRow {
     static constexpr int LB = sizeof(V) == 16 ? 3 : 4;
     static constexpr int G = 1 << LB;
     V* s;
+    __host__ __device__ static constexpr int ilog2(int v) { return v > 1 ? 1 + ilog2(v / 2) : 0; }
+    template <int Rp, int Ns> __device__ __forceinline__ static int phys_x(int pos)
+    {
+        const int a = pos >> LB;
+        if constexpr (Ns >= G || (Rp & (Rp - 1)) != 0 || (Ns & (Ns - 1)) != 0) {
+            return pos ^ (a & (G - 1));
+        } else if constexpr (Ns * Rp < G) {
+            return pos ^ ((a * Ns) & (G - 1));
+        } else {
+            return pos ^ (((a >> ilog2(Ns * Rp / G)) * Ns) & (G - 1));
+        }
+    }
     __device__ __forceinline__ static int phys(int pos) { return pos ^ ((pos >> LB) & (G - 1)); }
+    template <int Rp, int Ns> __device__ __forceinline__ void st(int pos, V v) { s[phys_x<Rp, Ns>(pos)] = v; }
+    template <int Rp, int Ns> __device__ __forceinline__ V ld(int pos) const { return s[phys_x<Rp, Ns>(pos)]; }
     __device__ __forceinline__ void st(int pos, V v) { s[phys(pos)] = v; }
     __device__ __forceinline__ V ld(int pos) const { return s[phys(pos)]; }
 };

@@ -48,6 +48,11 @@ template <typename T, int N> struct PencilGeom {
     static constexpr int THREADS = TPF * W;
     static constexpr size_t TW_BYTES = (size_t)N * sizeof(V2<T>);  // Stockham table (N-1 used)
     static constexpr size_t SMEM = TW_BYTES + (size_t)N * W * sizeof(V2<T>);
+    // FP32 dot passes also stage the tile's field-spectrum pencils ([N][W],
+    // interleaved like the exchange buffer) when that fits in shared memory
+    static constexpr size_t DK_BYTES = (size_t)N * W * sizeof(V2<T>);
+    static constexpr bool DK_SMEM = sizeof(T) == 4 && SMEM + DK_BYTES <= 227 * 1024;
+    static constexpr size_t SMEM_DOT = SMEM + (DK_SMEM ? DK_BYTES : 0);
 };
 
 // Elements per thread of the row (contiguous-axis) transforms of length NH:
@@ -110,6 +115,22 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// One level of a warp's recursive-halving sum of per-lane arrays: v[0..2H)
+// -> v[0..H) holding, for lanes with (lane & O), the upper half plus the
+// partner lane's upper half, else the lower halves.
+template <int N2, int O> __device__ __forceinline__ void halve_sums(double* v, int lane)
+{
+    constexpr int H = N2 / 2;
+    const bool up = (lane & O) != 0;
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        const double keep = up ? v[k + H] : v[k];
+        const double send = up ? v[k] : v[k + H];
+        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    }
+}
 
 // Stage WZ consecutive spectrum rows (first hv entries, rounded up to a
 // 16-byte multiple, which stays inside the row stride ss) into `stage`
@@ -581,7 +602,8 @@ enum SpecEpi : int {
 // r2max (sums only): no shell of the launch holds a mode with |m|^2 > r2max,
 // so a tile of pencils whose (my, mz) lie outside that ball is skipped.
 template <typename T, int N, bool DOT>
-__global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) == 8) ? 1 : 2)
+__global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
+                                  DOT ? (PencilGeom<T, N>::THREADS <= 256 ? 2 : 1) : (sizeof(T) == 8 ? 1 : 2))
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, int ndk, const Shell* __restrict__ shells,
             int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight, int quad,
@@ -607,12 +629,32 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
     if constexpr (!DOT) {
         if (jband < N / 2 && abs(my) > jband) return;  // rows outside the field's band
     }
+    const bool use_dk = epi == SPEC_DOT || epi == SPEC_DOT_ABS;
+    const size_t jdk = (size_t)(my < 0 ? my + ndk : my);
+    V* sdk = reinterpret_cast<V*>(smem_raw + G::SMEM);
     if constexpr (DOT) {
         // the whole tile outside every shell: no transform, zero partials
         const bool live = col_ok && my * my + mz * mz <= r2max;
         if (!__syncthreads_or(live)) {
             if (threadIdx.x < nshell) partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = 0.0;
             return;
+        }
+        if constexpr (G::DK_SMEM) {
+            // field-spectrum pencils of the tile (128 bytes per x row, rows
+            // that can hold a shell mode only) copied while the transform runs
+            if (use_dk) {
+                constexpr int EPC = 16 / (int)sizeof(V), CPR = G::W / EPC;
+                const int h0 = (blockIdx.x % tiles_per_row) * G::W;
+                const long long rest = (long long)r2max - (long long)my * my - (long long)h0 * h0;
+                for (int c = threadIdx.x; c < N * CPR; c += G::THREADS) {
+                    const int i = c / CPR, q = c - i * CPR;
+                    const int mx = lattice_freq(i, N);
+                    if ((long long)mx * mx <= rest)
+                        cp_async16(sdk + i * G::W + q * EPC,
+                                   dk + ((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h0 + q * EPC);
+                }
+            }
+            cp_async_commit();
         }
     }
     V a[G::R];
@@ -701,8 +743,10 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
         // Per-shell FP64 sums in registers, then one fixed-order reduction for
         // all shells at once (deterministic): warp xor-trees, per-warp rows in
         // shared memory, one thread per shell sums the rows in warp order.
-        const bool use_dk = epi == SPEC_DOT || epi == SPEC_DOT_ABS;
-        const size_t jdk = (size_t)(my < 0 ? my + ndk : my);
+        if constexpr (G::DK_SMEM) {
+            cp_async_wait_all();
+            __syncthreads();
+        }
         double acc[MAX_DOT_SHELLS];
 #pragma unroll
         for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = 0.0;
@@ -716,8 +760,13 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
             if (b) {
                 double val;
                 if (use_dk) {
-                    const int mx = lattice_freq(t + G::TPF * e, N);
-                    const V d = dk[((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h];
+                    V d;
+                    if constexpr (G::DK_SMEM) {
+                        d = sdk[(t + G::TPF * e) * G::W + w];
+                    } else {
+                        const int mx = lattice_freq(t + G::TPF * e, N);
+                        d = dk[((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h];
+                    }
                     val = wgt * ((double)d.x * (double)a[e].x + (double)d.y * (double)a[e].y);
                 } else {
                     val = wgt * rint((double)a[e].x * inv_n3);
@@ -728,16 +777,21 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS, (DOT || sizeof(T) =
                     if ((b >> c) & 1u) acc[c] += val;
             }
         }
+        // warp sums of the 16 shells by recursive halving: at lane offset o
+        // each lane keeps half of its shells (the upper half when lane & o)
+        // and adds the partner's copy of that half, so after offsets 16, 8,
+        // 4, 2 lane l holds one shell, c(l) = 8 b4 + 4 b3 + 2 b2 + b1 (b_k
+        // the lane bits), summed over 16 lanes; offset 1 completes it.
+        static_assert(MAX_DOT_SHELLS == 16, "halving tree of 16 shells");
         constexpr int NW = G::THREADS / 32;
         __shared__ double wsum[NW][MAX_DOT_SHELLS];
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-        for (int c = 0; c < MAX_DOT_SHELLS; c++) {
-            double v = acc[c];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == c) wsum[wid][c] = v;
-        }
+        halve_sums<16, 16>(acc, lane);
+        halve_sums<8, 8>(acc, lane);
+        halve_sums<4, 4>(acc, lane);
+        halve_sums<2, 2>(acc, lane);
+        acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 1);
+        if ((lane & 1) == 0) wsum[wid][(lane >> 1) & 15] = acc[0];
         __syncthreads();
         if (threadIdx.x < nshell) {
             double sum = 0.0;

@@ -151,8 +151,8 @@ template <typename T, int N> struct L3 {
         const unsigned blocks = (unsigned)(nj * (nc / PG::W));
         const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT || epi == SPEC_DOT_ABS;
         if (dot) {
-            PS_LTRY(set_smem(k_fwd_x<T, N, true>, PG::SMEM));
-            k_fwd_x<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(
+            PS_LTRY(set_smem(k_fwd_x<T, N, true>, PG::SMEM_DOT));
+            k_fwd_x<T, N, true><<<blocks, PG::THREADS, PG::SMEM_DOT, st>>>(
                 data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
                 weight, quad, r2max, partials, tb.twp, mod_out, nc, jband);
         } else {
