@@ -1,13 +1,14 @@
 """Build libpsgpu.so (sm_100a) in-tree.
 
-    python -m polyspectrum_b200.build [--force] [--ptxas-verbose]
+    python -m polyspectrum_b200.build [--force] [--ptxas-verbose] [--kbench]
 
 Each translation unit compiles in its own nvcc process (the FFT kernels are
 heavily unrolled); objects go to polyspectrum_b200/_build/, the shared library
 to polyspectrum_b200/libpsgpu.so.  The library links the CUDA runtime
 statically and depends on no torch symbol.  The command-line driver
 (driver/ps_run.c, plain C over the C-ABI) is linked against it as
-polyspectrum_b200/ps_run.
+polyspectrum_b200/ps_run.  --kbench also builds polyspectrum_b200/ps_kbench, a
+stand-alone timing harness of the hot passes (csrc/ps_kbench.cu).
 """
 from __future__ import annotations
 
@@ -25,6 +26,7 @@ OUT_DIR = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libpsgpu.so")
 DRIVER_SRC = os.path.join(PKG, "driver", "ps_run.c")
 DRIVER = os.path.join(PKG, "ps_run")
+KBENCH = os.path.join(PKG, "ps_kbench")
 SOURCES = ["ps_api.cu", "ps_inst_f32.cu", "ps_inst_f64.cu", "ps_noalloc.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -98,12 +100,23 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = False)
     return LIB
 
 
+def build_kbench() -> str:
+    """nvcc the stand-alone kernel timing harness (no library link)."""
+    tmp = KBENCH + ".tmp"
+    subprocess.run([nvcc(), *FLAGS, "-o", tmp, os.path.join(CSRC, "ps_kbench.cu")], check=True)
+    os.replace(tmp, KBENCH)
+    return KBENCH
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--ptxas-verbose", action="store_true")
+    ap.add_argument("--kbench", action="store_true")
     a = ap.parse_args()
     print(build(force=a.force, ptxas_verbose=a.ptxas_verbose))
+    if a.kbench:
+        print(build_kbench())
 
 
 if __name__ == "__main__":

@@ -1,0 +1,132 @@
+// ps_kbench: per-kernel CUDA-event times of the hot passes on synthetic data,
+// without a context: the forward transform of a 512^3 XHI_DENS field limited
+// to band 164 (r2c rows, Y pass, phase-storing X pass), then the FP32 field
+// part of one pair group on a 384-point alias-free sub-grid (leg bands 64 and
+// 96, 16 closing shells up to band 161: two masked inverse X + Y passes, the
+// pair kernel, the forward Y pass and the 16-shell dot pass) -- the shapes of
+// the largest group of the 64-configuration 512^3 theta sweep.  About 2.7 GB
+// on the device, so it is also the small case for full ncu captures of these
+// kernels.  Values are synthetic (unit-modulus spectra, uniform real grids),
+// so only times are meaningful.
+//
+//     python -m polyspectrum_b200.build --kbench
+//     polyspectrum_b200/ps_kbench [reps]
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include <cmath>
+#include "ps_launch.cuh"
+
+namespace ps {
+int launch_fail(cudaError_t e, const char* what)
+{
+    fprintf(stderr, "%s: %s\n", what, cudaGetErrorString(e));
+    return 1;
+}
+template struct L3<float, 384>;
+template struct L3<float, 512>;
+}
+using namespace ps;
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { fprintf(stderr, "%s:%d %s\n", __FILE__, __LINE__, cudaGetErrorString(e_)); exit(1);} } while (0)
+#define LT(x) do { if ((x) != 0) { fprintf(stderr, "launch failed %s:%d\n", __FILE__, __LINE__); exit(1);} } while (0)
+
+__global__ void k_fill(float2* p, size_t n, unsigned seed)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)i * 2654435761u ^ seed;
+        h ^= h >> 13; h *= 0x5bd1e995u; h ^= h >> 15;
+        const float a = 6.2831853f * (h & 0xffffff) / 16777216.0f;
+        p[i] = make_float2(cosf(a), sinf(a));
+    }
+}
+__global__ void k_fill_real(float* p, size_t n, unsigned seed)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)i * 2654435761u ^ seed;
+        h ^= h >> 13; h *= 0x5bd1e995u; h ^= h >> 15;
+        p[i] = (h & 0xffff) / 65536.0f;
+    }
+}
+template <int M> Tables<float> make_tables()
+{
+    std::vector<float2> hp(M), hr(M / 2), h(M);
+    L3<float, M>::host_tables(hp.data(), hr.data());
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int m = 0; m < M; m++) {
+        const long double a = two_pi * (long double)m / (long double)M;
+        h[m].x = (float)cosl(a);
+        h[m].y = (float)(-sinl(a));
+    }
+    float2 *a, *b, *c;
+    CK(cudaMalloc(&a, M * 8)); CK(cudaMalloc(&b, M / 2 * 8)); CK(cudaMalloc(&c, M * 8));
+    CK(cudaMemcpy(a, hp.data(), M * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b, hr.data(), M / 2 * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c, h.data(), M * 8, cudaMemcpyHostToDevice));
+    return Tables<float>{a, b, c};
+}
+static int rup(int a, int b) { return (a + b - 1) / b * b; }
+struct Timer {
+    std::vector<cudaEvent_t> ev; std::vector<double> acc; int k = 0;
+    Timer(int n) : ev(n + 1), acc(n, 0.0) { for (auto& e : ev) CK(cudaEventCreate(&e)); }
+    void start() { k = 0; CK(cudaEventRecord(ev[0])); }
+    void lap() { CK(cudaEventRecord(ev[++k])); }
+    void collect() { CK(cudaEventSynchronize(ev[k]));
+        for (int q = 0; q < k; q++) { float ms; CK(cudaEventElapsedTime(&ms, ev[q], ev[q + 1])); acc[q] += ms; } }
+};
+
+int main(int argc, char** argv)
+{
+    const int reps = argc > 1 ? atoi(argv[1]) : 10;
+    const int N = 512, SN = 272, hcols = 165, M = 384, ba = 64, bb = 96, bc = 161;
+    const size_t n3 = (size_t)N * N * N;
+    float *da, *db;
+    float2* spec;
+    CK(cudaMalloc(&da, n3 * 4)); CK(cudaMalloc(&db, n3 * 4));
+    CK(cudaMalloc(&spec, (size_t)N * N * SN * 8));
+    k_fill_real<<<1184, 256>>>(da, n3, 3u);
+    k_fill_real<<<1184, 256>>>(db, n3, 5u);
+    k_fill<<<1184, 256>>>(spec, (size_t)N * N * SN, 17u);
+    const int Sa = rup(ba + 1, 16), Sb = rup(bb + 1, 16), S = rup(bc + 1, 16);
+    float2 *wa, *wb, *w3;
+    CK(cudaMalloc(&wa, (size_t)M * M * Sa * 8)); CK(cudaMalloc(&wb, (size_t)M * M * Sb * 8)); CK(cudaMalloc(&w3, (size_t)M * M * S * 8));
+    Shell hs[2] = {};
+    const int bands[2] = {ba, bb};
+    for (int q = 0; q < 2; q++) { hs[q].kind = SHELL_RANGE; hs[q].band = bands[q]; hs[q].r2lo = (bands[q] - 2) * (bands[q] - 2); hs[q].r2hi = bands[q] * bands[q]; }
+    Shell* dsh; CK(cudaMalloc(&dsh, sizeof(hs))); CK(cudaMemcpy(dsh, hs, sizeof(hs), cudaMemcpyHostToDevice));
+    const int lut_size = bc * bc + 1;
+    std::vector<unsigned short> lut(lut_size, 0);
+    for (int c = 0; c < 16; c++) {
+        const double r = 32 + (bc - 34) * (c + 0.5) / 16.0;
+        for (int r2 = 0; r2 < lut_size; r2++) { const double s = std::sqrt((double)r2); if (s >= r - 2.5 && s <= r + 2.5) lut[r2] |= (unsigned short)(1u << c); }
+    }
+    unsigned short* dlut; CK(cudaMalloc(&dlut, lut_size * 2)); CK(cudaMemcpy(dlut, lut.data(), lut_size * 2, cudaMemcpyHostToDevice));
+    double* partials; CK(cudaMalloc(&partials, (size_t)M * 64 * 16 * sizeof(double)));
+    Tables<float> T5 = make_tables<512>(), T3 = make_tables<384>();
+    using L5 = L3<float, 512>;
+    using L4 = L3<float, 384>;
+    const char* names[] = {"fwd_z@512", "pass_y@512", "fwd_x_store@512", "inv_x A@384", "pass_y A@384", "inv_x B@384",
+                           "pass_y B@384", "pair_z@384", "pass_y fwd@384", "fwd_x_dot@384"};
+    const int NK = 10;
+    Timer tm(NK);
+    for (int it = 0; it < reps + 3; it++) {
+        tm.start();
+        LT(L5::fwd_z(0, SRC_XHI_F32, da, db, spec, SN, hcols, T5)); tm.lap();
+        LT(L5::pass_y(0, spec, SN, false, T5, 0, N, 176)); tm.lap();
+        LT(L5::fwd_x(0, spec, SN, hcols, SPEC_STORE_PHASE, spec, SN, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, T5,
+                     nullptr, 1.0, 0, 0, 0x7fffffff, nullptr, 176, 164)); tm.lap();
+        LT(L4::inv_x(0, spec, SN, wa, Sa, LOAD_MASKED, dsh, M / 2 + 1, T3, 0, N, 1)); tm.lap();
+        LT(L4::pass_y(0, wa, Sa, true, T3, 0, ba)); tm.lap();
+        LT(L4::inv_x(0, spec, SN, wb, Sb, LOAD_MASKED, dsh + 1, M / 2 + 1, T3, 0, N, 1)); tm.lap();
+        LT(L4::pass_y(0, wb, Sb, true, T3, 0, bb)); tm.lap();
+        LT(L4::pair_z(0, wa, Sa, ba + 1, wb, Sb, bb + 1, w3, S, bc + 1, T3)); tm.lap();
+        LT(L4::pass_y(0, w3, S, false, T3)); tm.lap();
+        int nb = 0;
+        LT(L4::fwd_x(0, w3, S, bc + 1, SPEC_DOT, nullptr, 0, spec, SN, nullptr, 16, dlut, lut_size, partials, T3, &nb,
+                     1.0, 0, N, lut_size - 1)); tm.lap();
+        CK(cudaGetLastError());
+        if (it == 2) { CK(cudaDeviceSynchronize()); tm.acc.assign(NK, 0.0); } else tm.collect();
+    }
+    CK(cudaDeviceSynchronize());
+    for (int q = 0; q < NK; q++) printf("%-18s %.4f ms\n", names[q], tm.acc[q] / reps);
+    return 0;
+}
