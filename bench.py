@@ -10,6 +10,7 @@ theta bins each = 64 bispectrum configurations with their polygon counts.
 A step runs the forward transform of the field and all 64 configurations.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--save-tune FILE | --tune-table FILE]
 
 Prints one JSON line (rank 0).  `value` is device-timed with inputs resident
 in HBM; `e2e` is the same step through the C-ABI from pinned host inputs with
@@ -235,8 +236,15 @@ def run_ours(args, rank, world, local_rank):
     xhii = torch.from_numpy(xhii_np).to(dev)
     # the 64 configurations planned once (transform size of each pair group
     # autotuned at planning); executions replay one CUDA graph
-    plan = ctx.plan(cfgs, method=ps.PS_FP32_BATCHED, graph=True, autotune=not args.no_autotune)
+    if args.tune_table:  # sub-grids fixed by an earlier run's table (profiling runs)
+        with open(args.tune_table) as f:
+            ctx.tune_import(f.read())
+    plan = ctx.plan(cfgs, method=ps.PS_FP32_BATCHED, graph=True,
+                    autotune=not (args.no_autotune or args.tune_table))
     tune_table = ctx.tune_export()
+    if args.save_tune and rank == 0:
+        with open(args.save_tune, "w") as f:
+            f.write(tune_table)
     # the field spectrum is computed up to the band the plan's shells reach
     # (every mode the 64 configurations read; results identical to a full load)
     spectrum_band = plan.band if not args.full_spectrum else -1
@@ -471,6 +479,9 @@ def main():
                     help="transform the field up to Nyquist instead of the plan's band")
     ap.add_argument("--no-autotune", action="store_true",
                     help="smallest alias-free sub-grid per pair group, no timing at planning")
+    ap.add_argument("--save-tune", default=None, help="write the plan's sub-grid table to this file")
+    ap.add_argument("--tune-table", default=None,
+                    help="take the sub-grids from a table written by --save-tune (no autotuning)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -539,7 +539,8 @@ int pair_spectrum(ps_gpu_ctx* c, const V2<T>* A, int Sa, int hba, const V2<T>* B
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, tb, quad))));
+        // rows |my| >= hout lie outside every shell the product is dotted with
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, tb, quad, NN, 0, hout - 1))));
         pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V, N);
     }
     *S_out = S;

@@ -104,13 +104,14 @@ int main(int argc, char** argv)
     Tables<float> T5 = make_tables<512>(), T3 = make_tables<384>();
     using L5 = L3<float, 512>;
     using L4 = L3<float, 384>;
-    const char* names[] = {"fwd_z@512", "pass_y@512", "fwd_x_store@512", "inv_x A@384", "pass_y A@384", "inv_x B@384",
+    const char* names[] = {"fwd_z@512 direct", "fwd_z@512 staged", "pass_y@512", "fwd_x_store@512", "inv_x A@384", "pass_y A@384", "inv_x B@384",
                            "pass_y B@384", "pair_z@384", "pass_y fwd@384", "fwd_x_dot@384"};
-    const int NK = 10;
+    const int NK = 11;
     Timer tm(NK);
     for (int it = 0; it < reps + 3; it++) {
         tm.start();
-        LT(L5::fwd_z(0, SRC_XHI_F32, da, db, spec, SN, hcols, T5)); tm.lap();
+        LT(L5::fwd_z(0, SRC_XHI_F32, da, db, spec, SN, hcols, T5, 0)); tm.lap();
+        LT(L5::fwd_z(0, SRC_XHI_F32, da, db, spec, SN, hcols, T5, 1)); tm.lap();
         LT(L5::pass_y(0, spec, SN, false, T5, 0, N, 176)); tm.lap();
         LT(L5::fwd_x(0, spec, SN, hcols, SPEC_STORE_PHASE, spec, SN, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, T5,
                      nullptr, 1.0, 0, 0, 0x7fffffff, nullptr, 176, 164)); tm.lap();
@@ -119,7 +120,7 @@ int main(int argc, char** argv)
         LT(L4::inv_x(0, spec, SN, wb, Sb, LOAD_MASKED, dsh + 1, M / 2 + 1, T3, 0, N, 1)); tm.lap();
         LT(L4::pass_y(0, wb, Sb, true, T3, 0, bb)); tm.lap();
         LT(L4::pair_z(0, wa, Sa, ba + 1, wb, Sb, bb + 1, w3, S, bc + 1, T3)); tm.lap();
-        LT(L4::pass_y(0, w3, S, false, T3)); tm.lap();
+        LT(L4::pass_y(0, w3, S, false, T3, 0, M, 0, bc)); tm.lap();
         int nb = 0;
         LT(L4::fwd_x(0, w3, S, bc + 1, SPEC_DOT, nullptr, 0, spec, SN, nullptr, 16, dlut, lut_size, partials, T3, &nb,
                      1.0, 0, N, lut_size - 1)); tm.lap();

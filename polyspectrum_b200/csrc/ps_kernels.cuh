@@ -239,7 +239,8 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 // ------------------------------------------------------------------ Y pass
 template <typename T, int N, bool INV>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
-    k_pass_y(V2<T>* __restrict__ data, int stride, int ncols, int quad, int jband, const V2<T>* __restrict__ tw_g)
+    k_pass_y(V2<T>* __restrict__ data, int stride, int ncols, int quad, int jband, int jout,
+             const V2<T>* __restrict__ tw_g)
 {
     using G = PencilGeom<T, N>;
     using V = V2<T>;
@@ -268,7 +269,8 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int j = t + G::TPF * e;
-        if (!quad || j <= N / 2) base[(size_t)j * stride] = a[e];
+        // jout < N/2: rows with |my| > jout are read by no later pass and not stored
+        if ((!quad || j <= N / 2) && (jout >= N / 2 || abs(lattice_freq(j, N)) <= jout)) base[(size_t)j * stride] = a[e];
     }
 }
 
@@ -486,13 +488,18 @@ __device__ __forceinline__ V2<T> load_pair(int kind, const unsigned char* ra, co
     }
 }
 
-// One tile per CTA (the input rows are dense and all loads are issued up front;
-// `vec`: the sources are aligned for one vector load per value pair).
-// FP32 rows of 512: at most 32 registers (no spill), so eight 256-thread CTAs
-// (every warp slot of the SM) keep their loads in flight; the pass is bound by
-// load latency.
-template <typename T, int N>
-__global__ void __launch_bounds__(RowGeom<T, N>::THREADS, (sizeof(T) == 4 && N == 512) ? 8 : 1)
+// One tile of WZ consecutive rows per CTA.  Two ways to bring the rows in:
+//  * STAGED: the tile's input bytes (contiguous: WZ rows of N values per input
+//    array) are copied to shared memory by cp.async (16-byte, L2-only) and the
+//    loader reads its value pairs from there, so no register holds a load in
+//    flight; FP32 rows of 512 then run four 256-thread CTAs per SM with up to
+//    64 registers.  Needs 16-byte aligned inputs of 4- or 8-byte values.
+//  * direct: all loads issued up front into registers (`vec`: one vector load
+//    per value pair); FP32 rows of 512 are held to 32 registers so that eight
+//    CTAs (every warp slot of the SM) keep their loads in flight.
+template <typename T, int N, bool STAGED>
+__global__ void __launch_bounds__(RowGeom<T, N>::THREADS,
+                                  (sizeof(T) == 4 && N == 512) ? (STAGED ? 4 : 8) : 1)
     k_fwd_z(int kind, const void* __restrict__ a_src, const void* __restrict__ b_src,
             V2<T>* __restrict__ dst, int dst_stride, int hout, int vec, const V2<T>* __restrict__ twr_g,
             const V2<T>* __restrict__ twpp_g)
@@ -503,27 +510,50 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS, (sizeof(T) == 4 && N =
     const int w0 = threadIdx.x / G::TPF, t0 = threadIdx.x % G::TPF;
     const size_t row = (size_t)blockIdx.x * G::WZ + w0;
     V a[G::R];
-    if (kind == SRC_T) {
-        const V* xr = reinterpret_cast<const V*>((const T*)a_src + row * N);
-#pragma unroll
-        for (int e = 0; e < G::R; e++) a[e] = xr[t0 + G::TPF * e];
-    } else if (vec) {
-        // both values of a pair in one 8- or 16-byte load per array
+    if constexpr (STAGED) {
         const int eb = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 4 : 8;
-        const unsigned char* ra = reinterpret_cast<const unsigned char*>(a_src) + row * N * eb;
-        const unsigned char* rb = b_src ? reinterpret_cast<const unsigned char*>(b_src) + row * N * eb : nullptr;
+        const size_t tile_bytes = (size_t)G::WZ * N * eb;
+        unsigned char* sa = smem_raw + G::STAGE_OFF;
+        unsigned char* sb = sa + tile_bytes;
+        const unsigned char* ga = reinterpret_cast<const unsigned char*>(a_src) + (size_t)blockIdx.x * tile_bytes;
+        const unsigned char* gb =
+            b_src ? reinterpret_cast<const unsigned char*>(b_src) + (size_t)blockIdx.x * tile_bytes : nullptr;
+        for (size_t c = threadIdx.x; c < tile_bytes / 16; c += G::THREADS) {
+            cp_async16(sa + 16 * c, ga + 16 * c);
+            if (gb) cp_async16(sb + 16 * c, gb + 16 * c);
+        }
+        cp_async_commit();
+        RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
+        cp_async_wait_all();
+        __syncthreads();
+        const unsigned char* ra = sa + (size_t)w0 * N * eb;
+        const unsigned char* rb = gb ? sb + (size_t)w0 * N * eb : nullptr;
 #pragma unroll
         for (int e = 0; e < G::R; e++) a[e] = load_pair<T>(kind, ra, rb, t0 + G::TPF * e);
+        r2c_row<T, N>(a, rc, dst + row * dst_stride, hout);
     } else {
+        if (kind == SRC_T) {
+            const V* xr = reinterpret_cast<const V*>((const T*)a_src + row * N);
 #pragma unroll
-        for (int e = 0; e < G::R; e++) {
-            const size_t n2 = row * N + 2 * (t0 + G::TPF * e);
-            a[e] = V{load_real<T>(kind, a_src, b_src, n2), load_real<T>(kind, a_src, b_src, n2 + 1)};
+            for (int e = 0; e < G::R; e++) a[e] = xr[t0 + G::TPF * e];
+        } else if (vec) {
+            // both values of a pair in one 8- or 16-byte load per array
+            const int eb = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 4 : 8;
+            const unsigned char* ra = reinterpret_cast<const unsigned char*>(a_src) + row * N * eb;
+            const unsigned char* rb = b_src ? reinterpret_cast<const unsigned char*>(b_src) + row * N * eb : nullptr;
+#pragma unroll
+            for (int e = 0; e < G::R; e++) a[e] = load_pair<T>(kind, ra, rb, t0 + G::TPF * e);
+        } else {
+#pragma unroll
+            for (int e = 0; e < G::R; e++) {
+                const size_t n2 = row * N + 2 * (t0 + G::TPF * e);
+                a[e] = V{load_real<T>(kind, a_src, b_src, n2), load_real<T>(kind, a_src, b_src, n2 + 1)};
+            }
         }
+        RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
+        __syncthreads();
+        r2c_row<T, N>(a, rc, dst + row * dst_stride, hout);
     }
-    RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
-    __syncthreads();
-    r2c_row<T, N>(a, rc, dst + row * dst_stride, hout);
 }
 
 // ------------------------------------------------------------------ pair Z

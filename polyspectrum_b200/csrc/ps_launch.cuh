@@ -87,18 +87,19 @@ template <typename T, int N> struct L3 {
     }
     // jband < N/2: input rows with |my| > jband are zero and are not read
     // ncols (0: stride): only columns h < ncols, a multiple of the pencil width
+    // jout < N/2: output rows with |my| > jout are not stored
     static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb, int quad = 0,
-                      int jband = N, int ncols = 0)
+                      int jband = N, int ncols = 0, int jout = N)
     {
         const int ni = quad ? N / 2 + 1 : N;
         const int nc = ncols > 0 ? ncols : stride;
         const unsigned blocks = (unsigned)(ni * (nc / PG::W));
         if (inv) {
             PS_LTRY(set_smem(k_pass_y<T, N, true>, PG::SMEM));
-            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, nc, quad, jband, tb.twp);
+            k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, nc, quad, jband, jout, tb.twp);
         } else {
             PS_LTRY(set_smem(k_pass_y<T, N, false>, PG::SMEM));
-            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, nc, quad, jband, tb.twp);
+            k_pass_y<T, N, false><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, nc, quad, jband, jout, tb.twp);
         }
         return PS_OK;
     }
@@ -114,16 +115,29 @@ template <typename T, int N> struct L3 {
         if (nblocks) *nblocks = grid;
         return PS_OK;
     }
+    // stage: 1 copies the input rows to shared memory first (k_fwd_z STAGED),
+    // 0 loads them straight into registers, -1 picks staging when it applies
+    // (16-byte aligned inputs of 4- or 8-byte values, tile fits shared memory)
     static int fwd_z(cudaStream_t st, int kind, const void* a, const void* b, V* dst, int ds, int hout,
-                     const Tables<T>& tb)
+                     const Tables<T>& tb, int stage = -1)
     {
-        constexpr size_t smem = RG::STAGE_OFF;
-        PS_LTRY(set_smem(k_fwd_z<T, N>, smem));
-        const unsigned blocks = (unsigned)((size_t)N * N / RG::WZ);
         const bool two = kind == SRC_XHI_F32 || kind == SRC_XHI_F64;
+        const size_t eb = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 4 : 8;
+        const uintptr_t addr = (uintptr_t)a | (two ? (uintptr_t)b : 0);
+        const size_t smem_staged = RG::STAGE_OFF + (two ? 2 : 1) * (size_t)RG::WZ * N * eb;
+        const bool can_stage = kind != SRC_T && addr % 16 == 0 && smem_staged <= 227 * 1024;
+        const unsigned blocks = (unsigned)((size_t)N * N / RG::WZ);
+        if (stage != 0 && can_stage) {
+            PS_LTRY(set_smem(k_fwd_z<T, N, true>, smem_staged));
+            k_fwd_z<T, N, true><<<blocks, RG::THREADS, smem_staged, st>>>(kind, a, b, dst, ds, hout, 1, tb.twr,
+                                                                           tb.twpp);
+            return PS_OK;
+        }
+        constexpr size_t smem = RG::STAGE_OFF;
+        PS_LTRY(set_smem(k_fwd_z<T, N, false>, smem));
         const uintptr_t need = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 8 : 16;  // float2 / double2
-        const int vec = kind != SRC_T && (((uintptr_t)a | (two ? (uintptr_t)b : 0)) % need) == 0;
-        k_fwd_z<T, N><<<blocks, RG::THREADS, smem, st>>>(kind, a, b, dst, ds, hout, vec, tb.twr, tb.twpp);
+        const int vec = kind != SRC_T && (addr % need) == 0;
+        k_fwd_z<T, N, false><<<blocks, RG::THREADS, smem, st>>>(kind, a, b, dst, ds, hout, vec, tb.twr, tb.twpp);
         return PS_OK;
     }
     static int pair_z(cudaStream_t st, const V* a, int sa, int hva, const V* b, int sb, int hvb, V* dst,
