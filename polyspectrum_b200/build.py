@@ -7,7 +7,8 @@ heavily unrolled); objects go to polyspectrum_b200/_build/, the shared library
 to polyspectrum_b200/libpsgpu.so.  The library links the CUDA runtime
 statically and depends on no torch symbol.  The command-line driver
 (driver/ps_run.c, plain C over the C-ABI) is linked against it as
-polyspectrum_b200/ps_run.  --kbench also builds polyspectrum_b200/ps_kbench, a
+polyspectrum_b200/ps_run, and the ini-file generator (driver/ps_create_ini.c) as
+polyspectrum_b200/ps_create_ini.  --kbench also builds polyspectrum_b200/ps_kbench, a
 stand-alone timing harness of the hot passes (csrc/ps_kbench.cu).
 """
 from __future__ import annotations
@@ -27,6 +28,8 @@ LIB = os.path.join(PKG, "libpsgpu.so")
 DRIVER_SRC = os.path.join(PKG, "driver", "ps_run.c")
 DRIVER = os.path.join(PKG, "ps_run")
 KBENCH = os.path.join(PKG, "ps_kbench")
+CREATE_INI_SRC = os.path.join(PKG, "driver", "ps_create_ini.c")
+CREATE_INI = os.path.join(PKG, "ps_create_ini")
 SOURCES = ["ps_api.cu", "ps_inst_f32.cu", "ps_inst_f64.cu", "ps_noalloc.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -62,7 +65,18 @@ def build_driver(force: bool = False) -> str:
     subprocess.run(["gcc", "-std=c99", "-O2", "-Wall", "-Wextra", "-o", tmp, DRIVER_SRC, "-L", PKG, "-lpsgpu",
                     "-Wl,-rpath,$ORIGIN", "-lm"], check=True)
     os.replace(tmp, DRIVER)
+    build_create_ini()
     return DRIVER
+
+
+def build_create_ini() -> str:
+    """gcc the ini-file generator (plain C, no library)."""
+    if os.path.exists(CREATE_INI) and os.path.getmtime(CREATE_INI) >= os.path.getmtime(CREATE_INI_SRC):
+        return CREATE_INI
+    tmp = CREATE_INI + ".tmp"
+    subprocess.run(["gcc", "-std=c99", "-O2", "-Wall", "-Wextra", "-o", tmp, CREATE_INI_SRC], check=True)
+    os.replace(tmp, CREATE_INI)
+    return CREATE_INI
 
 
 def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = False) -> str:

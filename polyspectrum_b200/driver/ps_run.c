@@ -328,6 +328,30 @@ static int write_output(const run_conf *c, const char *fname, int num, const dou
     return fclose(f) == 0 ? 0 : -1;
 }
 
+/* --exact: the same results at full precision ("%.17g": every double round-trips),
+   one line per configuration with its legs as the estimator used them (a
+   DERIVED closing leg with its computed range), written to <fname>.exact;
+   the reference's file keeps "%e" (6 digits). */
+static int write_exact(const run_conf *c, const char *fname, int num, const double *theta, const double *k,
+                       const ps_cfg *cfgs, const double *B, const double *Np)
+{
+    const size_t len = strlen(fname) + 7;
+    char *path = malloc(len);
+    snprintf(path, len, "%s.exact", fname);
+    FILE *f = fopen(path, "wb");
+    free(path);
+    if (!f) return -1;
+    fprintf(f, "# n = %d; per configuration: theta [rad], k [h Mpc^-1], then (k_i kmin_i kmax_i) per leg, "
+               "Polyspectrum_%d, Npolygons\n", c->n, c->n);
+    for (int i = 0; i < num; i++) {
+        fprintf(f, "%.17g\t%.17g", theta[i], k[i]);
+        for (int l = 0; l < cfgs[i].n; l++)
+            fprintf(f, "\t%.17g\t%.17g\t%.17g", cfgs[i].k[l], cfgs[i].kmin[l], cfgs[i].kmax[l]);
+        fprintf(f, "\t%.17g\t%.17g\n", B[i], Np[i]);
+    }
+    return fclose(f) == 0 ? 0 : -1;
+}
+
 static void die_ps(const char *what, int rc)
 {
     fprintf(stderr, "ps_run: %s: %s (%s)\n", what, ps_gpu_strerror(rc), ps_gpu_last_error());
@@ -338,14 +362,14 @@ static void usage(void)
 {
     printf("ps_run: B200 polyspectrum estimator\n");
     printf("USAGE:\n");
-    printf("ps_run [--method batched|plain] [--device D] [--dry-run] iniFile\n");
+    printf("ps_run [--method batched|plain] [--device D] [--dry-run] [--exact] iniFile\n");
     exit(EXIT_FAILURE);
 }
 
 int main(int argc, char **argv)
 {
     const double t1 = (double)time(NULL);
-    int method = PS_FP32_BATCHED, device = -1, dry = 0;
+    int method = PS_FP32_BATCHED, device = -1, dry = 0, exact = 0;
     const char *ini_path = NULL;
     for (int a = 1; a < argc; a++) {
         if (strcmp(argv[a], "--method") == 0 && a + 1 < argc) {
@@ -357,6 +381,8 @@ int main(int argc, char **argv)
             device = atoi(argv[++a]);
         } else if (strcmp(argv[a], "--dry-run") == 0) {
             dry = 1;
+        } else if (strcmp(argv[a], "--exact") == 0) {
+            exact = 1;
         } else if (argv[a][0] == '-' || ini_path) {
             usage();
         } else {
@@ -475,6 +501,10 @@ int main(int argc, char **argv)
     printf("FILENAME : %s\n", fname);
     if (write_output(&c, fname, num, th, kv, B, Np) != 0) {
         fprintf(stderr, "ps_run: cannot write %s\n", fname);
+        exit(EXIT_FAILURE);
+    }
+    if (exact && write_exact(&c, fname, num, th, kv, cfgs, B, Np) != 0) {
+        fprintf(stderr, "ps_run: cannot write %s.exact\n", fname);
         exit(EXIT_FAILURE);
     }
     ps_gpu_finalize(ctx);

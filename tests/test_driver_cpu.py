@@ -111,3 +111,76 @@ def test_usage(tools):
     import subprocess
     r = subprocess.run([PS_RUN], capture_output=True, text=True)
     assert r.returncode != 0 and "USAGE" in r.stdout
+
+
+# ---------------------------------------------------------------- ini-file generator
+CREATE_INI = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "polyspectrum_b200",
+                          "ps_create_ini")
+INI_ARGS = ["64", "100.3", "0", "1", "dens.raw", "xhii.raw", "0.7", "0.0456", "0.27", "0.73", "0.82", "0.24",
+            "XHI_DENS", "PHASE", "3", "0", "0.25", "0.3", "5", "0.1", "1.0", "DERIVED", "0.2", "out", "run", "1"]
+
+
+def _ini_args(phase):
+    """The generator's positional arguments (useOnlyPhase in slot 14 when given)."""
+    a = list(INI_ARGS)
+    if phase is None:
+        a.remove("PHASE")
+    else:
+        a[a.index("PHASE")] = str(phase)
+    return a
+
+
+@pytest.fixture(scope="module")
+def ini_tools():
+    from polyspectrum_b200 import build
+    build.build_create_ini()
+    ref_dir = os.path.join(os.path.dirname(oracle.__file__), "_ref")
+    if not os.path.exists(os.path.join(ref_dir, "create_inifile_phase")) and oracle.reference_checkout() is not None:
+        oracle.build_oracle(ref=True)
+    return ref_dir
+
+
+@pytest.mark.parametrize("phase", [None, 0, 1], ids=["no_phase_key", "phase0", "phase1"])
+def test_create_ini_matches_reference_generator(ini_tools, tmp_path, phase):
+    """Byte-for-byte the file of the reference's generator (main.c without the
+    useOnlyPhase argument, main_withOptionPhase.c with it)."""
+    import subprocess
+    ref_exe = os.path.join(ini_tools, "create_inifile" if phase is None else "create_inifile_phase")
+    if not os.path.exists(ref_exe):
+        pytest.skip("reference generators not built (needs the reference checkout at build time)")
+    args = _ini_args(phase)
+    ours = subprocess.run([CREATE_INI, str(tmp_path / "ours.ini"), *args], capture_output=True, text=True)
+    ref = subprocess.run([ref_exe, str(tmp_path / "ref.ini"), *args], capture_output=True, text=True)
+    assert ours.returncode == 0 and ref.returncode == 0, (ours.stderr, ref.stderr)
+    assert (tmp_path / "ours.ini").read_bytes() == (tmp_path / "ref.ini").read_bytes()
+
+
+def test_create_ini_wrong_argument_count(ini_tools, tmp_path):
+    """A wrong argument count is an error exit with the usage (the reference
+    writes through an uninitialised file name there)."""
+    import subprocess
+    r = subprocess.run([CREATE_INI, str(tmp_path / "x.ini"), "64"], capture_output=True, text=True)
+    assert r.returncode == 1 and "usage" in r.stderr
+    assert not (tmp_path / "x.ini").exists()
+
+
+def test_generated_ini_runs_like_reference(tools, ini_tools, tmp_path):
+    """A generated ini file drives ps_run --dry-run to the configurations and
+    output file name of the reference executable on the same file."""
+    import subprocess
+    make_run(str(tmp_path), n_grid=16, box=100.0)  # the inputs dens.raw / xhii.raw
+    args = _ini_args(1)
+    args[0], args[1] = "16", "100.0"
+    ini = str(tmp_path / "gen.ini")
+    assert subprocess.run([CREATE_INI, ini, *args]).returncode == 0
+    ref = oracle.run_ref_exe(ini, cwd=str(tmp_path))
+    assert ref.returncode == 0, ref.stderr
+    ours = run_driver(ini, "--dry-run", cwd=str(tmp_path))
+    assert ours.returncode == 0, ours.stderr
+    fname = output_file(ref.stdout)
+    assert output_file(ours.stdout) == fname
+    _, rows = text_columns(os.path.join(str(tmp_path), fname))
+    cfg = dry_run_configs(ours.stdout)
+    assert len(cfg) == len(rows) == 5
+    for (theta, k), row in zip(cfg, rows):
+        assert row[0] == "%e" % theta and row[1] == "%e" % k

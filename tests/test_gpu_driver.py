@@ -71,3 +71,36 @@ def test_driver_output_matches_reference(gpu_lib, ref_exe, tmp_path, name, metho
     # progress lines carry the same k values
     lines = [ln for ln in ours.stdout.splitlines() if ln.startswith(("k = ", "k1 = "))]
     assert len(lines) == len(rows)
+
+
+def test_driver_exact_sidecar(gpu_lib, ref_exe, tmp_path):
+    """ps_run --exact writes <output>.exact: the results at full precision
+    ("%.17g"), equal to the C-ABI's batch on the same field and configurations,
+    with the DERIVED closing ranges the estimator used; the reference-format
+    file beside it rounds the same numbers to "%e"."""
+    ps = gpu_lib
+    kw = dict(CASES["xhidens_mixed_precision_phase_derived"])
+    ini = make_run(str(tmp_path), n_grid=32, **kw)
+    ours = run_driver(ini, "--method", "plain", "--exact", cwd=str(tmp_path))
+    assert ours.returncode == 0, ours.stderr
+    fname = os.path.join(str(tmp_path), output_file(ours.stdout))
+    _, rows = read_rows(fname)
+    with open(fname + ".exact") as f:
+        ex = [[float(x) for x in ln.split("\t")] for ln in f.read().splitlines()[1:]]
+    assert len(ex) == len(rows) == kw["num_values"]
+    for r, e in zip(rows, ex):
+        assert "%e" % e[0] == r[0] and "%e" % e[1] == r[1]
+        assert "%e" % e[-2] == r[2] and "%e" % e[-1] == r[3]
+    # the same numbers through the C-ABI (double inputs, as ps_run widens mixed precision)
+    cfgs, _, _ = ps.read_params_to_kvectors(32, 200.0, 3, k1=kw["k1"], k2=kw["k2"], num_values=kw["num_values"],
+                                            kbinningCase=ps.PS_BIN_DERIVED)
+    dens = np.fromfile(os.path.join(str(tmp_path), "dens.raw"), dtype=np.float32).astype(np.float64)
+    xhii = np.fromfile(os.path.join(str(tmp_path), "xhii.raw"), dtype=np.float64)
+    with ps.Context(32, 200.0, methods=ps.PS_FP64_PLAIN) as ctx:
+        ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens.reshape(32, 32, 32), xhii.reshape(32, 32, 32), use_only_phase=1)
+        B, Np, _, out = ctx.batch(cfgs, ps.PS_FP64_PLAIN)
+    for i, e in enumerate(ex):
+        assert e[-2] == B[i] and e[-1] == Np[i]
+        legs = np.array(e[2:-2]).reshape(3, 3)
+        np.testing.assert_array_equal(legs[:, 1], list(out[i].kmin)[:3])
+        np.testing.assert_array_equal(legs[:, 2], list(out[i].kmax)[:3])
