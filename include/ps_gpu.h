@@ -112,6 +112,17 @@ int ps_gpu_create(ps_gpu_ctx **ctx, int nbins, double boxsize, int methods, int 
 int ps_gpu_set_field(ps_gpu_ctx *ctx, int which, const void *dens, const void *xhii,
                      int is_double, int mem, int use_only_phase);
 
+/* ps_gpu_set_field reading the raw input grids from files, as read_grid does
+ * (grid.c:122-228: N^3 float or double values in native byte order, the
+ * gasInputsInDoublePrecision / ionInputsInDoublePrecision of the ini file):
+ * each file streams through two 64 MiB page-locked buffers, the read of one
+ * chunk overlapping the upload of the other, so no host copy of the grid is
+ * made.  The path a field does not use may be NULL.  A float file beside a
+ * double one is widened (exactly) on the device, as the reference's double
+ * field holds it.  A missing or short file gives PS_ERR_IO. */
+int ps_gpu_set_field_files(ps_gpu_ctx *ctx, int which, const char *dens_path, int dens_double,
+                           const char *xhii_path, int xhii_double, int use_only_phase);
+
 /* ps_gpu_create + ps_gpu_set_field for a single field (DENS slot). */
 int ps_gpu_init(ps_gpu_ctx **ctx, int nbins, double boxsize, const void *field,
                 int field_is_double, int use_only_phase, int methods);

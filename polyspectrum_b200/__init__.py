@@ -84,6 +84,7 @@ def lib() -> C.CDLL:
     L.ps_gpu_plan_destroy.argtypes = [vp]
     L.ps_gpu_plan_destroy.restype = None
     L.ps_gpu_set_field_async.argtypes = [vp, ip, vp, vp, ip, ip, ip]
+    L.ps_gpu_set_field_files.argtypes = [vp, ip, C.c_char_p, ip, C.c_char_p, ip, ip]
     L.ps_gpu_plan_submit.argtypes = [vp, vp, dp, dp, dp, C.POINTER(ps_cfg)]
     L.ps_gpu_synchronize.argtypes = [vp]
     L.ps_gpu_launch_count.argtypes = [vp]
@@ -109,7 +110,8 @@ def lib() -> C.CDLL:
                  "ps_gpu_kernel_stats", "ps_gpu_plan_create", "ps_gpu_plan_execute",
                  "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize",
                  "ps_gpu_tune_export", "ps_gpu_tune_import", "ps_gpu_keep_modulus",
-                 "ps_gpu_set_spectrum_band", "ps_gpu_plan_band", "ps_gpu_plan_launch", "ps_gpu_plan_results"):
+                 "ps_gpu_set_spectrum_band", "ps_gpu_plan_band", "ps_gpu_plan_launch", "ps_gpu_plan_results",
+                 "ps_gpu_set_field_files"):
         getattr(L, name).restype = ip
     _lib = L
     return L
@@ -214,6 +216,14 @@ class Context:
         _check(lib().ps_gpu_set_field(self._h, which, pd, px, is_double, mem, use_only_phase))
 
     set_field = get_FT_field
+
+    def set_field_files(self, which: int, dens_path=None, dens_double: bool = False, xhii_path=None,
+                        xhii_double: bool = False, use_only_phase: int = 0):
+        """Load the field from raw grid files, streamed to the device in chunks
+        (ps_gpu_set_field_files); each file is float or double."""
+        enc = lambda p: None if p is None else os.fsencode(p)
+        _check(lib().ps_gpu_set_field_files(self._h, which, enc(dens_path), int(bool(dens_double)),
+                                            enc(xhii_path), int(bool(xhii_double)), use_only_phase))
 
     def set_field_async(self, which: int, dens=None, xhii=None, use_only_phase: int = 0):
         """get_FT_field queued behind the work already on the context

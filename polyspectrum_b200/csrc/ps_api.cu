@@ -134,6 +134,10 @@ struct ps_gpu_ctx {
     int slot = 0;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+    // file uploads (ps_gpu_set_field_files): two page-locked chunk buffers,
+    // ev_chunk[q] = the copy out of chunk buffer q is done
+    void* pin[2] = {nullptr, nullptr};
+    cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
     std::atomic<int> async_err{0};  // status of work whose results arrived in a host callback
     std::set<ps_gpu_plan*> plans;   // live plans (finalize releases their device memory)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1924,6 +1928,9 @@ int timed_end(ps_gpu_ctx* c)
 // are copied on the copy stream into one of two staging slots, the forward
 // transform waits for that copy on the compute stream, so the upload of the
 // next field overlaps the work still queued on the current one.
+int ensure_stage(ps_gpu_ctx* c, size_t bytes);
+int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, int use_only_phase, int s);
+
 int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int is_double, int mem,
                int use_only_phase)
 {
@@ -1936,20 +1943,7 @@ int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int
     const size_t bytes = n3 * (is_double ? 8 : 4);
     int s = -1;
     if (mem == PS_MEM_HOST) {
-        if (c->stage_bytes < bytes) {
-            // earlier uploads and the transforms reading them finish first
-            PS_CK(cudaStreamSynchronize(c->copy_stream));
-            PS_CK(cudaStreamSynchronize(c->stream));
-            for (int q = 0; q < 2; q++)
-                for (int r = 0; r < 2; r++) {
-                    cudaFree(c->stage[q][r]);
-                    c->stage[q][r] = nullptr;
-                }
-            c->stage_bytes = 0;
-            for (int q = 0; q < 2; q++)
-                for (int r = 0; r < 2; r++) PS_TRY(alloc_dev((unsigned char**)&c->stage[q][r], bytes));
-            c->stage_bytes = bytes;
-        }
+        PS_TRY(ensure_stage(c, bytes));
         s = c->slot;
         c->slot ^= 1;
         PS_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_free[s], 0));
@@ -1960,6 +1954,13 @@ int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int
         a = c->stage[s][0];
         if (b) b = c->stage[s][1];
     }
+    return transform_field(c, a, b, is_double, use_only_phase, s);
+}
+
+// The forward transform of a loaded field (device arrays a, b), then slot s
+// (if any) is released.
+int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, int use_only_phase, int s)
+{
     const int kind = b ? (is_double ? SRC_XHI_F64 : SRC_XHI_F32) : (is_double ? SRC_F64 : SRC_F32);
     c->use_only_phase = use_only_phase;
     c->f.have_spec = c->d.have_spec = false;
@@ -1968,6 +1969,64 @@ int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int
     if (s >= 0) PS_CK(cudaEventRecord(c->ev_free[s], c->stream));
     c->field_set = true;
     return PS_OK;
+}
+
+// Staging slots of at least `bytes` per array (device, two slots of two).
+int ensure_stage(ps_gpu_ctx* c, size_t bytes)
+{
+    if (c->stage_bytes >= bytes) return PS_OK;
+    // earlier uploads and the transforms reading them finish first
+    PS_CK(cudaStreamSynchronize(c->copy_stream));
+    PS_CK(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < 2; q++)
+        for (int r = 0; r < 2; r++) {
+            cudaFree(c->stage[q][r]);
+            c->stage[q][r] = nullptr;
+        }
+    c->stage_bytes = 0;
+    for (int q = 0; q < 2; q++)
+        for (int r = 0; r < 2; r++) PS_TRY(alloc_dev((unsigned char**)&c->stage[q][r], bytes));
+    c->stage_bytes = bytes;
+    return PS_OK;
+}
+
+constexpr size_t kFileChunk = (size_t)64 << 20;  // bytes per page-locked chunk buffer
+
+static __global__ void k_widen(const float* __restrict__ in, double* __restrict__ out, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+// `bytes` of a raw file into device memory `dev` on the copy stream through
+// the two chunk buffers: the read of one chunk overlaps the copy of the other.
+int upload_file(ps_gpu_ctx* c, const char* path, size_t bytes, void* dev)
+{
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(PS_ERR_IO, "cannot open %s", path);
+    int rc = PS_OK, q = 0;
+    for (size_t done = 0; done < bytes; q ^= 1) {
+        const size_t len = std::min(kFileChunk, bytes - done);
+        cudaError_t e = cudaEventSynchronize(c->ev_chunk[q]);  // chunk buffer q copied out
+        if (e != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "chunk copy: %s", cudaGetErrorString(e));
+            break;
+        }
+        const size_t got = fread(c->pin[q], 1, len, f);
+        if (got != len) {
+            rc = fail(PS_ERR_IO, "%s holds %zu of the %zu bytes of the grid", path, done + got, bytes);
+            break;
+        }
+        e = cudaMemcpyAsync((unsigned char*)dev + done, c->pin[q], len, cudaMemcpyHostToDevice, c->copy_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_chunk[q], c->copy_stream);
+        if (e != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "chunk upload: %s", cudaGetErrorString(e));
+            break;
+        }
+        done += len;
+    }
+    fclose(f);
+    return rc;
 }
 
 }  // namespace
@@ -2082,6 +2141,69 @@ int ps_gpu_set_field_async(ps_gpu_ctx* c, int which, const void* dens, const voi
     if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
     PS_CK(cudaSetDevice(c->device));
     return load_field(c, which, dens, xhii, is_double, mem, use_only_phase);
+}
+
+int ps_gpu_set_field_files(ps_gpu_ctx* c, int which, const char* dens_path, int dens_double, const char* xhii_path,
+                           int xhii_double, int use_only_phase)
+{
+    g_err[0] = 0;
+    if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
+    if (which < PS_FIELD_DENS || which > PS_FIELD_XHI_DENS) return fail(PS_ERR_ARG, "which=%d", which);
+    const bool use_d = which != PS_FIELD_XHII, use_x = which != PS_FIELD_DENS;
+    if ((use_d && !dens_path) || (use_x && !xhii_path)) return fail(PS_ERR_ARG, "input file name is NULL");
+    PS_CK(cudaSetDevice(c->device));
+    PS_TRY(timed_begin(c));
+    // the field's precision: double when any file it reads holds doubles (a
+    // float file beside it is widened exactly on the device)
+    const int dp = (use_d && dens_double) || (use_x && xhii_double);
+    const size_t n3 = (size_t)c->N * c->N * c->N;
+    PS_TRY(ensure_stage(c, n3 * (dp ? 8 : 4)));
+    for (int q = 0; q < 2; q++) {
+        if (!c->pin[q] && cudaHostAlloc(&c->pin[q], kFileChunk, cudaHostAllocDefault) != cudaSuccess) {
+            c->pin[q] = nullptr;
+            return fail(PS_ERR_OOM, "page-locked chunk buffer of %zu bytes", kFileChunk);
+        }
+        if (!c->ev_chunk[q]) PS_CK(cudaEventCreateWithFlags(&c->ev_chunk[q], cudaEventDisableTiming));
+    }
+    const int s = c->slot;
+    c->slot ^= 1;
+    PS_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_free[s], 0));
+    struct Input {
+        const char* path;
+        int is_double;
+    };
+    Input in[2];
+    int nin = 0;
+    if (which == PS_FIELD_XHII) in[nin++] = {xhii_path, xhii_double};
+    else in[nin++] = {dens_path, dens_double};
+    if (which == PS_FIELD_XHI_DENS) in[nin++] = {xhii_path, xhii_double};
+    int rc = PS_OK;
+    for (int r = 0; r < nin && rc == PS_OK; r++) {
+        if (in[r].is_double || !dp) {
+            rc = upload_file(c, in[r].path, n3 * (in[r].is_double ? 8 : 4), c->stage[s][r]);
+        } else {
+            // a float file of a double field: through the other slot's array (after
+            // the transform that last read it), widened into this slot
+            cudaError_t e = cudaStreamWaitEvent(c->copy_stream, c->ev_free[s ^ 1], 0);
+            if (e != cudaSuccess) rc = fail(PS_ERR_CUDA, "%s", cudaGetErrorString(e));
+            if (rc == PS_OK) rc = upload_file(c, in[r].path, n3 * 4, c->stage[s ^ 1][r]);
+            if (rc == PS_OK) {
+                k_widen<<<148 * 8, 256, 0, c->copy_stream>>>((const float*)c->stage[s ^ 1][r], (double*)c->stage[s][r],
+                                                             n3);
+                e = cudaGetLastError();
+                if (e != cudaSuccess) rc = fail(PS_ERR_CUDA, "widen: %s", cudaGetErrorString(e));
+            }
+        }
+    }
+    if (rc != PS_OK) {
+        cudaStreamSynchronize(c->copy_stream);  // no copy still reads a chunk buffer
+        return rc;
+    }
+    PS_CK(cudaEventRecord(c->ev_copied[s], c->copy_stream));
+    PS_CK(cudaStreamWaitEvent(c->stream, c->ev_copied[s], 0));
+    PS_TRY(transform_field(c, c->stage[s][0], nin > 1 ? c->stage[s][1] : nullptr, dp, use_only_phase, s));
+    PS_CK(cudaStreamSynchronize(c->copy_stream));
+    return timed_end(c);
 }
 
 int ps_gpu_init(ps_gpu_ctx** ctx, int nbins, double boxsize, const void* field, int field_is_double,
@@ -2530,6 +2652,8 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
         for (int r = 0; r < 2; r++) cudaFree(c->stage[q][r]);
         if (c->ev_copied[q]) cudaEventDestroy(c->ev_copied[q]);
         if (c->ev_free[q]) cudaEventDestroy(c->ev_free[q]);
+        if (c->pin[q]) cudaFreeHost(c->pin[q]);
+        if (c->ev_chunk[q]) cudaEventDestroy(c->ev_chunk[q]);
     }
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);

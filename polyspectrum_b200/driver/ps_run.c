@@ -252,41 +252,36 @@ static void read_conf(const char *path, run_conf *c)
 
 /* ------------------------------------------------------------ inputs ----- */
 /* read_grid / read_grid_doubleprecision (grid.c:122-228): N^3 raw values */
-static void *read_raw(const char *path, size_t n3, int dp)
+/* An input grid file (read_grid, grid.c:122-228): it must hold n3 values of
+   its precision; returns the first value (the reference's progress line
+   prints the first value of the field).  The library then streams the file
+   to the device (ps_gpu_set_field_files). */
+static double check_raw(const char *path, size_t n3, int dp)
 {
     const size_t es = dp ? sizeof(double) : sizeof(float);
-    void *buf = malloc(n3 * es);
-    if (!buf) {
-        fprintf(stderr, "ps_run: no memory for %s\n", path);
-        exit(EXIT_FAILURE);
-    }
     FILE *f = fopen(path, "rb");
     if (!f) {
         fprintf(stderr, "ps_run: cannot open input file %s\n", path);
         exit(EXIT_FAILURE);
     }
-    const size_t got = fread(buf, es, n3, f);
+    double v = 0.0;
+    size_t got = 0;
+    if (dp) got = fread(&v, es, 1, f);
+    else {
+        float x = 0.f;
+        got = fread(&x, es, 1, f);
+        v = (double)x;
+    }
+    long long size = -1;
+    if (fseek(f, 0, SEEK_END) == 0) size = (long long)ftell(f);
     fclose(f);
-    if (got != n3) {
-        fprintf(stderr, "ps_run: %s holds %zu of the %zu values of the grid\n", path, got, n3);
+    const size_t have = size >= 0 ? (size_t)size / es : got;
+    if (got != 1 || have < n3) {
+        fprintf(stderr, "ps_run: %s holds %zu of the %zu values of the grid\n", path, have < n3 ? have : 0, n3);
         exit(EXIT_FAILURE);
     }
-    return buf;
+    return v;
 }
-
-static double *to_double(float *a, size_t n3)
-{
-    double *d = malloc(n3 * sizeof(double));
-    if (!d) {
-        fprintf(stderr, "ps_run: no memory\n");
-        exit(EXIT_FAILURE);
-    }
-    for (size_t i = 0; i < n3; i++) d[i] = (double)a[i];
-    free(a);
-    return d;
-}
-
-static double first_value(const void *a, int dp) { return dp ? ((const double *)a)[0] : (double)((const float *)a)[0]; }
 
 /* ------------------------------------------------------------ output ----- */
 /* file name of save_polyspectrum(_numpolygons) (run.c:128-150) */
@@ -457,25 +452,14 @@ int main(int argc, char **argv)
     }
     printf("Option: %s\t", c.which_field);
     const size_t n3 = (size_t)c.grid_size * c.grid_size * c.grid_size;
-    void *dens = NULL, *xhii = NULL;
-    int dp = 0;
     double v0 = 0.0;
     if (which == PS_FIELD_DENS) {
-        dens = read_raw(c.density_file, n3, c.gas_dp == 1);
-        dp = c.gas_dp == 1;
-        v0 = first_value(dens, dp);
+        v0 = check_raw(c.density_file, n3, c.gas_dp == 1);
     } else if (which == PS_FIELD_XHII) {
-        xhii = read_raw(c.ion_file, n3, c.ion_dp == 1);
-        dp = c.ion_dp == 1;
-        v0 = first_value(xhii, dp);
+        v0 = check_raw(c.ion_file, n3, c.ion_dp == 1);
     } else {
-        dens = read_raw(c.density_file, n3, c.gas_dp == 1);
-        xhii = read_raw(c.ion_file, n3, c.ion_dp == 1);
-        v0 = first_value(dens, c.gas_dp == 1) * (1. - first_value(xhii, c.ion_dp == 1));  /* input_field.c:33 */
-        dp = c.gas_dp == 1 || c.ion_dp == 1;
-        /* mixed precision: the float grid is widened (exactly) to double */
-        if (dp && c.gas_dp != 1) dens = to_double(dens, n3);
-        if (dp && c.ion_dp != 1) xhii = to_double(xhii, n3);
+        const double d0 = check_raw(c.density_file, n3, c.gas_dp == 1);
+        v0 = d0 * (1. - check_raw(c.ion_file, n3, c.ion_dp == 1)); /* input_field.c:33 */
     }
     printf(" Mean value from FT is %e\nComputing FFT... ", v0);
     fflush(stdout);
@@ -483,11 +467,10 @@ int main(int argc, char **argv)
     ps_gpu_ctx *ctx = NULL;
     rc = ps_gpu_create(&ctx, c.grid_size, (double)(float)c.box_size, method, device);  /* grid.h:9 */
     if (rc) die_ps("context", rc);
-    rc = ps_gpu_set_field(ctx, which, dens, xhii, dp, PS_MEM_HOST, c.calc_phases_only == 1);
+    rc = ps_gpu_set_field_files(ctx, which, which == PS_FIELD_XHII ? NULL : c.density_file, c.gas_dp == 1,
+                                which == PS_FIELD_DENS ? NULL : c.ion_file, c.ion_dp == 1, c.calc_phases_only == 1);
     if (rc) die_ps("field", rc);
     printf("done.\n");
-    free(dens);
-    free(xhii);
 
     rc = ps_gpu_polyspectrum_batch(ctx, method, num, cfgs, B, Np, NULL);
     if (rc) die_ps("polyspectrum", rc);

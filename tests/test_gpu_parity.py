@@ -445,3 +445,39 @@ def test_plan_launch_and_results(gpu_lib):
     np.testing.assert_array_equal(Np, want[1])
     for i in range(len(cfgs)):
         assert list(out[i].kmin)[:3] == list(want[3][i].kmin)[:3]
+
+
+@pytest.mark.parametrize("layout", ["xhidens_f32", "xhidens_mixed", "xhii_f64", "dens_f32"])
+def test_field_files_match_set_field(gpu_lib, tmp_path, layout):
+    """Grids streamed from raw files (ps_gpu_set_field_files: chunked through
+    page-locked buffers, a float file beside a double one widened on the
+    device) give exactly the results of the same grids passed as arrays; a
+    short file is an I/O error."""
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    dens, xhii = fields(n_grid, box)
+    dens = (1.0 + dens.astype(np.float64))
+    which, d_dp, x_dp = {"xhidens_f32": (2, 0, 0), "xhidens_mixed": (2, 0, 1), "xhii_f64": (1, 0, 1),
+                         "dens_f32": (0, 0, 0)}[layout]
+    d_arr = dens if d_dp else dens.astype(np.float32)
+    x_arr = xhii.astype(np.float64) if x_dp else xhii.astype(np.float32)
+    d_arr.tofile(tmp_path / "dens.raw")
+    x_arr.tofile(tmp_path / "xhii.raw")
+    dp = (which != 1 and d_dp) or (which != 0 and x_dp)
+    as_field = lambda a: a.astype(np.float64) if dp else a
+    cfgs, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=0.1, k2=0.14, num_values=4, kbinningCase=1)
+    with ps.Context(n_grid, box) as ctx:
+        ctx.get_FT_field(which, as_field(d_arr) if which != 1 else None, as_field(x_arr) if which != 0 else None,
+                         use_only_phase=1)
+        want = [ctx.batch(cfgs, m)[:2] for m in (ps.PS_FP64_PLAIN, ps.PS_FP32_BATCHED)]
+        ctx.set_field_files(which, str(tmp_path / "dens.raw") if which != 1 else None, d_dp,
+                            str(tmp_path / "xhii.raw") if which != 0 else None, x_dp, use_only_phase=1)
+        got = [ctx.batch(cfgs, m)[:2] for m in (ps.PS_FP64_PLAIN, ps.PS_FP32_BATCHED)]
+        for (Bw, Nw), (Bg, Ng) in zip(want, got):
+            np.testing.assert_array_equal(Bg, Bw)
+            np.testing.assert_array_equal(Ng, Nw)
+        short = tmp_path / "short.raw"
+        d_arr.ravel()[:100].tofile(short)
+        with pytest.raises(ps.PsError) as e:
+            ctx.set_field_files(0, str(short), d_dp, None, 0, use_only_phase=1)
+        assert e.value.status == -3
