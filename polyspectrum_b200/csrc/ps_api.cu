@@ -1458,11 +1458,12 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
     if (nd > 0) {
         ops.push_back([=]() {
             PS_CK(cudaMemcpyAsync(dmm, dmm_init, 16 * (size_t)nd, cudaMemcpyDeviceToDevice, c->stream));
-            for (int q = 0; q < nd; q++) {
-                const int band = std::min(derived[q].band, N / 2);
-                const int blocks = derived_blocks(derived[q], band);
+            int blocks = 1;  // all shells in one launch, sized for the largest
+            for (int q = 0; q < nd; q++)
+                blocks = std::max(blocks, derived_blocks(derived[q], std::min(derived[q].band, N / 2)));
+            {
                 Prof pf(c);
-                k_derived_range<<<blocks, 256, 0, c->stream>>>(N, dderived + q, band, dmm + 2 * q);
+                k_derived_ranges<<<dim3(blocks, nd), 256, 0, c->stream>>>(N, dderived, dmm);
                 pf.end(KF_DERIVED, 0.0);
             }
             Prof pf(c);

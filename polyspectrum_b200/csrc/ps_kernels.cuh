@@ -1008,10 +1008,28 @@ __device__ __forceinline__ int isqrt_floor(int v)  // floor(sqrt(v)), v >= 0
     return r;
 }
 
+// DERIVED range of one shell: min/max of the squared corner radii over its
+// modes with |mz| <= hmax, folded into minmax_bits[0..1] (bit patterns of
+// non-negative doubles order as integers).  The grid's x extent strides the
+// shell's modes.
+__device__ __forceinline__ void derived_range_body(int n, const Shell& sh, int hmax, unsigned long long* minmax_bits);
+
 static __global__ void k_derived_range(int n, const Shell* __restrict__ shell_p, int hmax,
                                        unsigned long long* minmax_bits)
 {
-    const Shell sh = *shell_p;
+    derived_range_body(n, *shell_p, hmax, minmax_bits);
+}
+
+// nd shells in one launch: blockIdx.y selects the shell (hmax = its band, at
+// most n/2); blocks past what a shell needs find no mode and fold nothing.
+static __global__ void k_derived_ranges(int n, const Shell* __restrict__ shells, unsigned long long* minmax_bits)
+{
+    const Shell sh = shells[blockIdx.y];
+    derived_range_body(n, sh, min(sh.band, n / 2), minmax_bits + 2 * blockIdx.y);
+}
+
+__device__ __forceinline__ void derived_range_body(int n, const Shell& sh, int hmax, unsigned long long* minmax_bits)
+{
     const int band = min(sh.band, n / 2);
     const int side = 2 * band + 1;
     double min2 = sh.min2_init, max2 = 0.0;
