@@ -94,6 +94,25 @@ def test_unknown_field(tools, tmp_path):
     assert ours.stdout.splitlines()[-1].startswith("Option: RHO")
 
 
+@pytest.mark.parametrize("what", ["short", "missing"])
+def test_input_file_errors(tools, tmp_path, what):
+    """A short or missing input grid ends the run with an error before any
+    device is touched (ps_run checks each file's size and first value, then
+    the library streams it)."""
+    ini = make_run(str(tmp_path), n_grid=16, which=2, gas_dp=0, ion_dp=1)
+    path = tmp_path / "xhii.raw"
+    if what == "short":
+        data = path.read_bytes()
+        path.write_bytes(data[: len(data) // 2])
+    else:
+        path.unlink()
+    ours = run_driver(ini, cwd=str(tmp_path))
+    assert ours.returncode != 0
+    msg = ("xhii.raw holds 2048 of the 4096 values of the grid" if what == "short"
+           else "cannot open input file xhii.raw")
+    assert msg in ours.stderr
+
+
 def test_n_above_three(tools, tmp_path):
     ref, ours = _both(tmp_path, ("--dry-run",), n=4)
     assert ref.returncode != 0 and ours.returncode != 0
