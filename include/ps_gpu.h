@@ -187,6 +187,16 @@ void ps_gpu_plan_destroy(ps_gpu_plan *plan);
  * the device during a submission are returned by ps_gpu_synchronize. */
 int ps_gpu_set_field_async(ps_gpu_ctx *ctx, int which, const void *dens, const void *xhii,
                            int is_double, int mem, int use_only_phase);
+/* Host XHI_DENS float inputs of a context created with PS_FP32_BATCHED alone
+ * (ps_gpu_set_field and ps_gpu_set_field_async): host threads compose
+ * dens*(1 - xHII), as input_field.c:33 computes it, for part of the rows into
+ * a library-owned page-locked buffer, uploaded chunk by chunk at half the
+ * PCIe bytes, while the other rows go up as they are (from page-locked
+ * inputs only; pageable inputs are composed in full).  The split follows the
+ * measured compose and copy rates.  Results are bit-identical to the
+ * two-array upload.  ps_gpu_upload_bytes gives the host -> device bytes of
+ * the last host field load (no reference counterpart). */
+long long ps_gpu_upload_bytes(const ps_gpu_ctx *ctx);
 int ps_gpu_plan_submit(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
                        double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
 int ps_gpu_synchronize(ps_gpu_ctx *ctx);

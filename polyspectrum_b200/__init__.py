@@ -85,6 +85,8 @@ def lib() -> C.CDLL:
     L.ps_gpu_plan_destroy.restype = None
     L.ps_gpu_set_field_async.argtypes = [vp, ip, vp, vp, ip, ip, ip]
     L.ps_gpu_set_field_files.argtypes = [vp, ip, C.c_char_p, ip, C.c_char_p, ip, ip]
+    L.ps_gpu_upload_bytes.argtypes = [vp]
+    L.ps_gpu_upload_bytes.restype = C.c_longlong
     L.ps_gpu_plan_submit.argtypes = [vp, vp, dp, dp, dp, C.POINTER(ps_cfg)]
     L.ps_gpu_synchronize.argtypes = [vp]
     L.ps_gpu_launch_count.argtypes = [vp]
@@ -245,6 +247,10 @@ class Context:
             _check(lib().ps_gpu_synchronize(self._h))
         finally:
             self._inflight = []
+
+    def upload_bytes(self) -> int:
+        """Host -> device bytes of the last host field load (ps_gpu_upload_bytes)."""
+        return int(lib().ps_gpu_upload_bytes(self._h))
 
     def launch_count(self) -> int:
         """Kernels executed by this context since its creation."""

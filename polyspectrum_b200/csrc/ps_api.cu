@@ -1,5 +1,6 @@
 // libpsgpu: C-ABI, context, launch plumbing and the two estimator methods.
 #include <math.h>
+#include <sched.h>
 #include <stdarg.h>
 
 #include <cmath>
@@ -8,11 +9,13 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <atomic>
 #include <functional>
 #include <map>
 #include <set>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -138,6 +141,17 @@ struct ps_gpu_ctx {
     // ev_chunk[q] = the copy out of chunk buffer q is done
     void* pin[2] = {nullptr, nullptr};
     cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
+    // XHI_DENS composed on the host (FP32-only contexts): two page-locked field
+    // buffers, ev_fpin[q] = the upload out of buffer q is done
+    void* fpin[2] = {nullptr, nullptr};
+    size_t fpin_bytes = 0;
+    int fslot = 0;
+    cudaEvent_t ev_fpin[2] = {nullptr, nullptr};
+    size_t upload_bytes = 0;  // host -> device bytes of the last host field load
+    // split of a host XHI_DENS load between raw rows (PCIe) and composed rows
+    // (host threads): the raw fraction and the measured seconds per row
+    double raw_frac = 0.3, t_comp_row = 0.0, t_up_row = 0.0;
+    cudaEvent_t ev_raw[2] = {nullptr, nullptr};
     std::atomic<int> async_err{0};  // status of work whose results arrived in a host callback
     std::set<ps_gpu_plan*> plans;   // live plans (finalize releases their device memory)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -576,7 +590,9 @@ int r2c_work(ps_gpu_ctx* c, int kind, const void* a, const void* b, int hout, in
 }
 
 // Forward field transform into B.spec (+ phase normalisation).
-template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, const void* b)
+// split > 0 (FP32 XHI_DENS host loads): rows [0, split) hold dens in a and
+// xHII in b, rows [split, N^2) the composed field in a (same offsets).
+template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, const void* b, size_t split = 0)
 {
     PrecBufs<T>& B = bufs<T>(c);
     const int N = c->N;
@@ -595,7 +611,16 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     const double src_bytes = kind == SRC_F32 ? 4.0 : kind == SRC_F64 ? 8.0 : kind == SRC_XHI_F32 ? 8.0 : 16.0;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, hcols, B.tables()))));
+        if (split == 0) {
+            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, hcols, B.tables()))));
+        } else {
+            const size_t nr = (size_t)N * N;
+            const float* af = (const float*)a;
+            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, SRC_XHI_F32, af, b, B.spec, B.S, hcols, B.tables(),
+                                                    -1, split))));
+            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, SRC_F32, af + split * N, nullptr,
+                                                    B.spec + split * B.S, B.S, hcols, B.tables(), -1, nr - split))));
+        }
         pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * H * V, N);
     }
     {
@@ -1930,7 +1955,121 @@ int timed_end(ps_gpu_ctx* c)
 // transform waits for that copy on the compute stream, so the upload of the
 // next field overlaps the work still queued on the current one.
 int ensure_stage(ps_gpu_ctx* c, size_t bytes);
-int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, int use_only_phase, int s);
+int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, int use_only_phase, int s,
+                    size_t split = 0);
+
+// dens * (1 - xhii) rounded to float, each value exactly as the r2c loader
+// computes it (double product and difference, input_field.c:33, then one
+// rounding), on host threads.
+void compose_xhi_dens(const float* d, const float* x, float* out, size_t n)
+{
+    // the CPUs this process may run on (a container's cpuset), at most 64
+    cpu_set_t set;
+    CPU_ZERO(&set);
+    const int ncpu = sched_getaffinity(0, sizeof(set), &set) == 0 ? CPU_COUNT(&set) : 1;
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(std::min(ncpu, 64), std::max<size_t>(1, n >> 18)));
+    auto work = [=](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; i++) out[i] = (float)((double)d[i] * (1.0 - (double)x[i]));
+    };
+    std::vector<std::thread> pool;
+    const size_t per = (n + nt - 1) / nt;
+    for (size_t t = 1; t < nt; t++) pool.emplace_back(work, std::min(n, t * per), std::min(n, (t + 1) * per));
+    work(0, std::min(n, per));
+    for (auto& th : pool) th.join();
+}
+
+// Host XHI_DENS field of an FP32-only context.  The first `split` rows go up
+// as they are (dens and xHII, the copy engine starts on them at once) while
+// host threads compose dens*(1 - xHII) of the other rows, chunk by chunk, into
+// one of two page-locked buffers, each chunk uploaded as soon as it is done:
+// composed rows cross PCIe at half the bytes, raw rows cost no host time, and
+// the split is re-balanced after every load from the measured compose and
+// copy rates (raw rows only from page-locked inputs).  Every composed value
+// equals the r2c loader's, so the spectrum and all results are bit-identical
+// to the two-array upload.
+int load_xhi_dens_host(ps_gpu_ctx* c, const float* dens, const float* xhii, int use_only_phase)
+{
+    const int N = c->N;
+    const size_t nr = (size_t)N * N, n3 = nr * N;
+    const size_t bytes = n3 * sizeof(float);
+    if (c->fpin_bytes < bytes) {
+        for (int q = 0; q < 2; q++) {
+            if (c->ev_fpin[q]) PS_CK(cudaEventSynchronize(c->ev_fpin[q]));
+            if (c->fpin[q]) cudaFreeHost(c->fpin[q]);
+            c->fpin[q] = nullptr;
+        }
+        c->fpin_bytes = 0;
+        for (int q = 0; q < 2; q++)
+            if (cudaHostAlloc(&c->fpin[q], bytes, cudaHostAllocDefault) != cudaSuccess) {
+                c->fpin[q] = nullptr;
+                return fail(PS_ERR_OOM, "page-locked field buffer of %zu bytes", bytes);
+            }
+        c->fpin_bytes = bytes;
+    }
+    for (int q = 0; q < 2; q++)
+        if (!c->ev_fpin[q]) PS_CK(cudaEventCreateWithFlags(&c->ev_fpin[q], cudaEventDisableTiming));
+    if (!c->ev_raw[0])
+        for (int q = 0; q < 2; q++) PS_CK(cudaEventCreate(&c->ev_raw[q]));
+    PS_TRY(ensure_stage(c, bytes));
+    // raw rows only when both inputs are page-locked (a pageable copy would
+    // hold the host thread until it is done)
+    auto pinned = [](const void* p) {
+        cudaPointerAttributes at;
+        return cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    };
+    const bool raw_ok = pinned(dens) && pinned(xhii);
+    cudaGetLastError();  // a pageable pointer may leave an error from the query
+    constexpr size_t kAlign = 64;  // rows per split step (a multiple of every r2c row tile)
+    size_t split = raw_ok ? (size_t)(c->raw_frac * (double)nr) / kAlign * kAlign : 0;
+    split = std::min(split, nr);
+    const int q = c->fslot;
+    c->fslot ^= 1;
+    PS_CK(cudaEventSynchronize(c->ev_fpin[q]));  // the upload that last read buffer q
+    const int s = c->slot;
+    c->slot ^= 1;
+    PS_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_free[s], 0));
+    float* d0 = (float*)c->stage[s][0];
+    float* d1 = (float*)c->stage[s][1];
+    float* hp = (float*)c->fpin[q];
+    if (split > 0) {
+        PS_CK(cudaEventRecord(c->ev_raw[0], c->copy_stream));
+        PS_CK(cudaMemcpyAsync(d0, dens, split * N * sizeof(float), cudaMemcpyHostToDevice, c->copy_stream));
+        PS_CK(cudaMemcpyAsync(d1, xhii, split * N * sizeof(float), cudaMemcpyHostToDevice, c->copy_stream));
+        PS_CK(cudaEventRecord(c->ev_raw[1], c->copy_stream));
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    // composed rows in 8 uploads: each chunk's copy overlaps the next chunk's composition
+    const size_t chunk = std::max<size_t>(kAlign, ((nr - split + 7) / 8 + kAlign - 1) / kAlign * kAlign);
+    for (size_t r0 = split; r0 < nr; r0 += chunk) {
+        const size_t r1 = std::min(nr, r0 + chunk);
+        compose_xhi_dens(dens + r0 * N, xhii + r0 * N, hp + r0 * N, (r1 - r0) * N);
+        PS_CK(cudaMemcpyAsync(d0 + r0 * N, hp + r0 * N, (r1 - r0) * N * sizeof(float), cudaMemcpyHostToDevice,
+                              c->copy_stream));
+    }
+    const double t_comp = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    PS_CK(cudaEventRecord(c->ev_fpin[q], c->copy_stream));
+    PS_CK(cudaEventRecord(c->ev_copied[s], c->copy_stream));
+    PS_CK(cudaStreamWaitEvent(c->stream, c->ev_copied[s], 0));
+    c->upload_bytes = (2 * split * N + (nr - split) * N) * sizeof(float);
+    PS_TRY(transform_field(c, d0, split > 0 ? d1 : nullptr, 0, use_only_phase, s, split));
+    // re-balance: with a composed rows at tc per row and every row's upload at
+    // tu per float row (raw rows move two), the load takes about
+    // max(tc (nr - split), tu (nr + split)); equal when split/nr = (tc - tu)/(tc + tu)
+    if (raw_ok) {
+        if (split < nr) c->t_comp_row = t_comp / (double)(nr - split);
+        if (split > 0) {
+            float ms = 0.f;
+            if (cudaEventSynchronize(c->ev_raw[1]) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, c->ev_raw[0], c->ev_raw[1]) == cudaSuccess && ms > 0.f)
+                c->t_up_row = 1e-3 * ms / (2.0 * (double)split);
+        }
+        if (c->t_comp_row > 0.0 && c->t_up_row > 0.0) {
+            const double f = (c->t_comp_row - c->t_up_row) / (c->t_comp_row + c->t_up_row);
+            c->raw_frac = std::min(0.95, std::max(0.0, f));
+        }
+    }
+    return PS_OK;
+}
 
 int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int is_double, int mem,
                int use_only_phase)
@@ -1943,7 +2082,10 @@ int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int
     const size_t n3 = (size_t)c->N * c->N * c->N;
     const size_t bytes = n3 * (is_double ? 8 : 4);
     int s = -1;
+    if (mem == PS_MEM_HOST && which == PS_FIELD_XHI_DENS && !is_double && c->methods == PS_FP32_BATCHED)
+        return load_xhi_dens_host(c, (const float*)dens, (const float*)xhii, use_only_phase);
     if (mem == PS_MEM_HOST) {
+        c->upload_bytes = bytes * (b ? 2 : 1);
         PS_TRY(ensure_stage(c, bytes));
         s = c->slot;
         c->slot ^= 1;
@@ -1960,12 +2102,13 @@ int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int
 
 // The forward transform of a loaded field (device arrays a, b), then slot s
 // (if any) is released.
-int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, int use_only_phase, int s)
+int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, int use_only_phase, int s,
+                    size_t split)
 {
-    const int kind = b ? (is_double ? SRC_XHI_F64 : SRC_XHI_F32) : (is_double ? SRC_F64 : SRC_F32);
+    const int kind = split ? SRC_F32 : b ? (is_double ? SRC_XHI_F64 : SRC_XHI_F32) : (is_double ? SRC_F64 : SRC_F32);
     c->use_only_phase = use_only_phase;
     c->f.have_spec = c->d.have_spec = false;
-    if (c->methods & PS_FP32_BATCHED) PS_TRY(forward_field<float>(c, kind, a, b));
+    if (c->methods & PS_FP32_BATCHED) PS_TRY(forward_field<float>(c, kind, a, b, split));
     if (c->methods & PS_FP64_PLAIN) PS_TRY(forward_field<double>(c, kind, a, b));
     if (s >= 0) PS_CK(cudaEventRecord(c->ev_free[s], c->stream));
     c->field_set = true;
@@ -2143,6 +2286,8 @@ int ps_gpu_set_field_async(ps_gpu_ctx* c, int which, const void* dens, const voi
     PS_CK(cudaSetDevice(c->device));
     return load_field(c, which, dens, xhii, is_double, mem, use_only_phase);
 }
+
+long long ps_gpu_upload_bytes(const ps_gpu_ctx* c) { return c ? (long long)c->upload_bytes : PS_ERR_ARG; }
 
 int ps_gpu_set_field_files(ps_gpu_ctx* c, int which, const char* dens_path, int dens_double, const char* xhii_path,
                            int xhii_double, int use_only_phase)
@@ -2655,6 +2800,9 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
         if (c->ev_free[q]) cudaEventDestroy(c->ev_free[q]);
         if (c->pin[q]) cudaFreeHost(c->pin[q]);
         if (c->ev_chunk[q]) cudaEventDestroy(c->ev_chunk[q]);
+        if (c->fpin[q]) cudaFreeHost(c->fpin[q]);
+        if (c->ev_fpin[q]) cudaEventDestroy(c->ev_fpin[q]);
+        if (c->ev_raw[q]) cudaEventDestroy(c->ev_raw[q]);
     }
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);

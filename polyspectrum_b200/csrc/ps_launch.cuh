@@ -118,15 +118,18 @@ template <typename T, int N> struct L3 {
     // stage: 1 copies the input rows to shared memory first (k_fwd_z STAGED),
     // 0 loads them straight into registers, -1 picks staging when it applies
     // (16-byte aligned inputs of 4- or 8-byte values, tile fits shared memory)
+    // nrows (0: all N^2): rows processed, from the row the pointers start at
+    // (a multiple of the row tile RG::WZ)
     static int fwd_z(cudaStream_t st, int kind, const void* a, const void* b, V* dst, int ds, int hout,
-                     const Tables<T>& tb, int stage = -1)
+                     const Tables<T>& tb, int stage = -1, size_t nrows = 0)
     {
         const bool two = kind == SRC_XHI_F32 || kind == SRC_XHI_F64;
         const size_t eb = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 4 : 8;
         const uintptr_t addr = (uintptr_t)a | (two ? (uintptr_t)b : 0);
         const size_t smem_staged = RG::STAGE_OFF + (two ? 2 : 1) * (size_t)RG::WZ * N * eb;
         const bool can_stage = kind != SRC_T && addr % 16 == 0 && smem_staged <= 227 * 1024;
-        const unsigned blocks = (unsigned)((size_t)N * N / RG::WZ);
+        const unsigned blocks = (unsigned)((nrows ? nrows : (size_t)N * N) / RG::WZ);
+        if (blocks == 0) return PS_OK;
         if (stage != 0 && can_stage) {
             PS_LTRY(set_smem(k_fwd_z<T, N, true>, smem_staged));
             k_fwd_z<T, N, true><<<blocks, RG::THREADS, smem_staged, st>>>(kind, a, b, dst, ds, hout, 1, tb.twr,

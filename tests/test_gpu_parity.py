@@ -481,3 +481,39 @@ def test_field_files_match_set_field(gpu_lib, tmp_path, layout):
         with pytest.raises(ps.PsError) as e:
             ctx.set_field_files(0, str(short), d_dp, None, 0, use_only_phase=1)
         assert e.value.status == -3
+
+
+@pytest.mark.parametrize("methods", ["fp32_only", "both"])
+def test_host_xhi_dens_composition(gpu_lib, methods):
+    """Host float XHI_DENS inputs of an FP32-only context are composed on the
+    host and uploaded as one float array (ps_gpu_upload_bytes = N^3 * 4);
+    with both methods the two arrays go up (2 N^3 * 4).  Either way the
+    results equal, bit for bit, those of the same arrays resident on the device
+    (composed by the r2c loader), synchronous and asynchronous loads alike."""
+    import torch
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    dens, xhii = field_args(2, *fields(n_grid, box))
+    m = ps.PS_FP32_BATCHED if methods == "fp32_only" else ps.PS_FP32_BATCHED | ps.PS_FP64_PLAIN
+    cfgs, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=0.1, k2=0.14, num_values=5, kbinningCase=1)
+    with ps.Context(n_grid, box, methods=m) as ctx:
+        ctx.get_FT_field(2, torch.from_numpy(dens).cuda(), torch.from_numpy(xhii).cuda(), use_only_phase=1)
+        want = ctx.batch(cfgs, ps.PS_FP32_BATCHED)[:2]
+        ctx.get_FT_field(2, dens, xhii, use_only_phase=1)
+        assert ctx.upload_bytes() == n_grid ** 3 * 4 * (1 if methods == "fp32_only" else 2)
+        got = ctx.batch(cfgs, ps.PS_FP32_BATCHED)[:2]
+        ctx.set_field_async(2, dens, xhii, use_only_phase=1)
+        ctx.synchronize()
+        got_async = ctx.batch(cfgs, ps.PS_FP32_BATCHED)[:2]
+        # page-locked inputs: part of the rows go up as they are, the rest composed
+        dp, xp = torch.from_numpy(dens).pin_memory(), torch.from_numpy(xhii).pin_memory()
+        got_pinned = []
+        for _ in range(3):  # the split is re-balanced after every load
+            ctx.set_field_async(2, dp, xp, use_only_phase=1)
+            ctx.synchronize()
+            up = ctx.upload_bytes()
+            assert n_grid ** 3 * 4 <= up <= 2 * n_grid ** 3 * 4
+            got_pinned.append(ctx.batch(cfgs, ps.PS_FP32_BATCHED)[:2])
+    for g in [got, got_async] + got_pinned:
+        np.testing.assert_array_equal(g[0], want[0])
+        np.testing.assert_array_equal(g[1], want[1])
