@@ -15,6 +15,8 @@
 #include <map>
 #include <set>
 #include <string>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 #include <tuple>
 #include <vector>
@@ -96,6 +98,62 @@ template <typename T> struct PrecBufs {
     std::map<int, std::array<V2<T>*, 3>> sub;
 };
 
+// Host worker threads (one per CPU this process may run on, at most 64),
+// started once per context: run(f) calls f(t) on every worker t and returns
+// when all are done.
+struct HostPool {
+    std::vector<std::thread> th;
+    std::mutex m;
+    std::condition_variable cv, done_cv;
+    std::function<void(size_t)> job;
+    size_t gen = 0, pending = 0, n = 1;
+    bool stop = false;
+    HostPool()
+    {
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        const int ncpu = sched_getaffinity(0, sizeof(set), &set) == 0 ? CPU_COUNT(&set) : 1;
+        n = (size_t)std::max(1, std::min(ncpu, 64));
+        for (size_t t = 1; t < n; t++)
+            th.emplace_back([this, t]() {
+                size_t seen = 0;
+                for (;;) {
+                    std::unique_lock<std::mutex> lk(m);
+                    cv.wait(lk, [&]() { return stop || gen != seen; });
+                    if (stop) return;
+                    seen = gen;
+                    const std::function<void(size_t)> f = job;
+                    lk.unlock();
+                    f(t);
+                    lk.lock();
+                    if (--pending == 0) done_cv.notify_one();
+                }
+            });
+    }
+    void run(const std::function<void(size_t)>& f)
+    {
+        {
+            std::lock_guard<std::mutex> lk(m);
+            job = f;
+            pending = n - 1;
+            ++gen;
+        }
+        cv.notify_all();
+        f(0);
+        std::unique_lock<std::mutex> lk(m);
+        done_cv.wait(lk, [&]() { return pending == 0; });
+    }
+    ~HostPool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(m);
+            stop = true;
+        }
+        cv.notify_all();
+        for (auto& t : th) t.join();
+    }
+};
+
 struct ps_gpu_ctx {
     int N = 0;
     double L = 0.0;  // (double)(float) box size, grid.h:9
@@ -151,6 +209,7 @@ struct ps_gpu_ctx {
     // split of a host XHI_DENS load between raw rows (PCIe) and composed rows
     // (host threads): the raw fraction and the measured seconds per row
     double raw_frac = 0.3, t_comp_row = 0.0, t_up_row = 0.0;
+    HostPool* pool = nullptr;  // host threads of the composition, made on first use
     cudaEvent_t ev_raw[2] = {nullptr, nullptr};
     std::atomic<int> async_err{0};  // status of work whose results arrived in a host callback
     std::set<ps_gpu_plan*> plans;   // live plans (finalize releases their device memory)
@@ -1961,21 +2020,14 @@ int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, 
 // dens * (1 - xhii) rounded to float, each value exactly as the r2c loader
 // computes it (double product and difference, input_field.c:33, then one
 // rounding), on host threads.
-void compose_xhi_dens(const float* d, const float* x, float* out, size_t n)
+void compose_xhi_dens(ps_gpu_ctx* c, const float* d, const float* x, float* out, size_t n)
 {
-    // the CPUs this process may run on (a container's cpuset), at most 64
-    cpu_set_t set;
-    CPU_ZERO(&set);
-    const int ncpu = sched_getaffinity(0, sizeof(set), &set) == 0 ? CPU_COUNT(&set) : 1;
-    const size_t nt = std::max<size_t>(1, std::min<size_t>(std::min(ncpu, 64), std::max<size_t>(1, n >> 18)));
-    auto work = [=](size_t lo, size_t hi) {
+    if (!c->pool) c->pool = new HostPool();
+    const size_t nt = c->pool->n, per = (n + nt - 1) / nt;
+    c->pool->run([=](size_t t) {
+        const size_t lo = std::min(n, t * per), hi = std::min(n, lo + per);
         for (size_t i = lo; i < hi; i++) out[i] = (float)((double)d[i] * (1.0 - (double)x[i]));
-    };
-    std::vector<std::thread> pool;
-    const size_t per = (n + nt - 1) / nt;
-    for (size_t t = 1; t < nt; t++) pool.emplace_back(work, std::min(n, t * per), std::min(n, (t + 1) * per));
-    work(0, std::min(n, per));
-    for (auto& th : pool) th.join();
+    });
 }
 
 // Host XHI_DENS field of an FP32-only context.  The first `split` rows go up
@@ -2042,7 +2094,7 @@ int load_xhi_dens_host(ps_gpu_ctx* c, const float* dens, const float* xhii, int 
     const size_t chunk = std::max<size_t>(kAlign, ((nr - split + 7) / 8 + kAlign - 1) / kAlign * kAlign);
     for (size_t r0 = split; r0 < nr; r0 += chunk) {
         const size_t r1 = std::min(nr, r0 + chunk);
-        compose_xhi_dens(dens + r0 * N, xhii + r0 * N, hp + r0 * N, (r1 - r0) * N);
+        compose_xhi_dens(c, dens + r0 * N, xhii + r0 * N, hp + r0 * N, (r1 - r0) * N);
         PS_CK(cudaMemcpyAsync(d0 + r0 * N, hp + r0 * N, (r1 - r0) * N * sizeof(float), cudaMemcpyHostToDevice,
                               c->copy_stream));
     }
@@ -2804,6 +2856,7 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
         if (c->ev_fpin[q]) cudaEventDestroy(c->ev_fpin[q]);
         if (c->ev_raw[q]) cudaEventDestroy(c->ev_raw[q]);
     }
+    delete c->pool;
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
