@@ -2067,10 +2067,13 @@ int load_xhi_dens_host(ps_gpu_ctx* c, const float* dens, const float* xhii, int 
     // hold the host thread until it is done)
     auto pinned = [](const void* p) {
         cudaPointerAttributes at;
-        return cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeHost;
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();  // the failed query's own error, not a kernel's
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
     };
     const bool raw_ok = pinned(dens) && pinned(xhii);
-    cudaGetLastError();  // a pageable pointer may leave an error from the query
     constexpr size_t kAlign = 64;  // rows per split step (a multiple of every r2c row tile)
     size_t split = raw_ok ? (size_t)(c->raw_frac * (double)nr) / kAlign * kAlign : 0;
     split = std::min(split, nr);
