@@ -284,17 +284,21 @@ int ps_gpu_set_profiling(ps_gpu_ctx *ctx, int on);
 int ps_gpu_kernel_stats(ps_gpu_ctx *ctx, ps_kernel_stat *out, int max);
 
 /* Power spectrum P(k) (n = 2, DEFAULT binning, one shell per k) of a field
- * that is already in device memory, without allocating anything: for callers
- * that may not call cudaMalloc (code running during CUDA stream capture, or a
- * host whose GPU memory belongs to another allocator).  No counterpart in the
+ * that is already in device memory, without allocating anything: for host
+ * programs whose GPU memory belongs to another allocator (a framework's
+ * caching pool that has reserved the device, a fixed real-time memory budget),
+ * where a library may not call cudaMalloc of its own.  No counterpart in the
  * reference.  field_dev: N^3 float32 on the current device; N must be 16, 32
- * or 64 and nshell 1..256, anything larger is rejected with PS_ERR_ARG.
+ * or 64, nshell 1..256, box size and kbinwidth positive and finite,
+ * use_only_phase 0 or 1; anything else is rejected with PS_ERR_ARG.
  * Results equal those of ps_gpu_polyspectrum_batch (PS_FP32_BATCHED) on the
  * configurations {n=2, k = {k[s], k[s]}}: P[s] = B, Npoly[s] = exact count.
  * Its working memory is one fixed 8 MiB device array that every GPU loading
  * the library holds until exit; all calls on a device share it, so calls that
- * overlap on the GPU race.  The first call on a device resolves the array's
- * address and should come before any stream capture.  stream may be NULL. */
+ * overlap on the GPU race.  The call reads its results back into P and Npoly
+ * and synchronises `stream` (NULL: the legacy default stream) before it
+ * returns.  The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture. */
 int ps_gpu_power_spectrum_noalloc(int nbins, double boxsize, const float *field_dev,
                                   int use_only_phase, int nshell, const double *k,
                                   double kbinwidth, double *P, double *Npoly, void *stream);

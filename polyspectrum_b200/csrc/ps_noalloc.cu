@@ -1,13 +1,14 @@
 // ps_gpu_power_spectrum_noalloc: the power spectrum P(k) of a device-resident
 // field without any device allocation.
 //
-// Who needs it: callers that are not allowed to call cudaMalloc - code running
-// while a stream is being captured into a CUDA graph (cudaMalloc is illegal
-// during capture), and hosts whose GPU memory is owned by another allocator
-// (a framework's caching pool, a fixed real-time budget) where a library may
-// not grab memory of its own.  Everything the computation needs beyond the
-// caller's input field and output arrays lives in one file-scope device array
-// of fixed size, reserved when the library is loaded.
+// Who needs it: host programs whose GPU memory is owned by another allocator
+// and may not be taken by a library behind its back - a framework's caching
+// pool that has reserved the device's memory for itself, or a real-time or
+// embedded host with a fixed, pre-planned memory budget - where a cudaMalloc
+// of the library's own would fail or break that budget.  Everything the
+// computation needs beyond the caller's input field and output arrays lives
+// in one file-scope device array of fixed size, which the CUDA runtime
+// reserves when it loads the library's device code.
 //
 // Limits and sharing:
 //   * grids up to PS_NOALLOC_MAX_N^3 (64^3), at most PS_NOALLOC_MAX_SHELLS
@@ -16,9 +17,12 @@
 //   * all calls on a device share the array and leave their data in it; calls
 //     that overlap on the GPU (different streams, or host threads without
 //     ordering between them) race on it - serialise them;
+//   * the call copies its small tables from host memory, reads its results
+//     back and synchronises `stream` before it returns;
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture begins.
+#include <cmath>
 #include <mutex>
 
 #include "ps_launch.cuh"
@@ -174,7 +178,11 @@ extern "C" int ps_gpu_power_spectrum_noalloc(int nbins, double boxsize, const fl
                                         "(the fixed scratch holds at most 64^3)");
     if (nshell < 1 || nshell > PS_NOALLOC_MAX_SHELLS)
         return report_error(PS_ERR_ARG, "ps_gpu_power_spectrum_noalloc: 1..256 shells per call");
-    if (!(boxsize > 0.0)) return report_error(PS_ERR_ARG, "box size must be positive");
+    if (!(boxsize > 0.0) || !std::isfinite(boxsize))
+        return report_error(PS_ERR_ARG, "box size must be positive and finite");
+    if (!(kbinwidth > 0.0) || !std::isfinite(kbinwidth))
+        return report_error(PS_ERR_ARG, "kbinwidth must be positive and finite");
+    if (use_only_phase != 0 && use_only_phase != 1) return report_error(PS_ERR_ARG, "use_only_phase must be 0 or 1");
     int dev = 0;
     PS_LCK(cudaGetDevice(&dev));
     unsigned char* base = nullptr;
