@@ -34,17 +34,17 @@ _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 
 
+# Where the build container keeps the read-only reference checkout; the GPU
+# hosts have none (they run the prebuilt oracle/_ref).  $PS_REFERENCE_DIR
+# overrides it.
+_DEFAULT_REFERENCE = "/root/reference"
+
+
 def reference_checkout() -> str | None:
-    """The reference checkout the Makefile's `ref` target compiles (its REF
-    variable, or $PS_REFERENCE_DIR), if it is present on this machine."""
-    path = os.environ.get("PS_REFERENCE_DIR")
-    if not path:
-        with open(os.path.join(HERE, "Makefile")) as f:
-            for line in f:
-                if line.startswith("REF ?="):
-                    path = line.split("?=", 1)[1].strip()
-                    break
-    return path if path and os.path.isdir(os.path.join(path, "src")) else None
+    """The reference checkout the Makefile's `ref` target compiles
+    ($PS_REFERENCE_DIR, else the build container's checkout), if present."""
+    path = os.environ.get("PS_REFERENCE_DIR") or _DEFAULT_REFERENCE
+    return path if os.path.isdir(os.path.join(path, "src")) else None
 
 
 def build_oracle(ref: bool = False) -> None:
@@ -158,7 +158,7 @@ def oracle_lib() -> C.CDLL:
         lib.ora_num_configs.argtypes = [C.POINTER(_OraParams)]
         lib.ora_num_configs.restype = C.c_int
         lib.ora_run.argtypes = [C.POINTER(_OraParams), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
-                                _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+                                C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         lib.ora_run.restype = C.c_int
         _ora = lib
     return _ora
@@ -226,18 +226,21 @@ def ora_num_polygons(n, legs_k, kmin, kmax, binwidth, binning, boxsize):
     return oracle_lib().ora_num_polygons(n, len(k), k, lo, hi, binwidth, binning, boxsize)
 
 
-def ora_run(p: RunParams, dens, xhii=None, max_cfg: int | None = None) -> RunResult:
+def ora_run(p: RunParams, dens, xhii=None, max_cfg: int | None = None, first: int = 0) -> RunResult:
+    """Configurations [first, first + max_cfg) of the run (all from `first`
+    when max_cfg is None), as the reference's run loop computes them."""
     lib = oracle_lib()
     cp = p.to_c()
     ncfg = lib.ora_num_configs(C.byref(cp))
     if ncfg < 0:
         raise ValueError("configuration refused by the reference's kvectors (n>3 or n<2)")
+    ncfg = max(0, ncfg - first)
     if max_cfg is not None:
         ncfg = min(ncfg, max_cfg)
     which = p.which_field
     (pd, px), is_double, keep = _fields_arg(which, dens, xhii)
     out = [np.zeros(ncfg) for _ in range(4)] + [np.zeros(ncfg * p.n) for _ in range(3)]
-    got = lib.ora_run(C.byref(cp), pd, px, is_double, ncfg, *out)
+    got = lib.ora_run(C.byref(cp), pd, px, is_double, first, ncfg, *out)
     del keep
     if got < 0:
         raise RuntimeError("ora_run failed")
@@ -274,6 +277,23 @@ def ref_lib() -> C.CDLL:
         lib.ref_run_ini.restype = C.c_int
         _ref = lib
     return _ref
+
+
+def ref_set_threads(n: int) -> None:
+    """Threads of the FFT shim inside oracle/_ref (0: $PS_SHIM_THREADS, else
+    every CPU)."""
+    lib = ref_lib()
+    lib.ps_shim_set_threads.argtypes = [C.c_int]
+    lib.ps_shim_set_threads.restype = None
+    lib.ps_shim_set_threads(int(n))
+
+
+def ora_set_threads(n: int) -> None:
+    """Threads of the FFT shim inside the restatement's library."""
+    lib = oracle_lib()
+    lib.ps_shim_set_threads.argtypes = [C.c_int]
+    lib.ps_shim_set_threads.restype = None
+    lib.ps_shim_set_threads(int(n))
 
 
 def write_ini(path: str, p: RunParams, dens_file: str, ion_file: str, is_double: int,

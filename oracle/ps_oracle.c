@@ -318,7 +318,7 @@ int ora_num_configs(const ora_params *p)
     return -1; /* kvectors.c:60-64, :140-144: refused */
 }
 
-int ora_run(const ora_params *p, const void *dens, const void *xhii, int is_double, int max_cfg,
+int ora_run(const ora_params *p, const void *dens, const void *xhii, int is_double, int first, int max_cfg,
             double *k_out, double *theta_out, double *B_out, double *npoly_out, double *kpoly_out,
             double *kmin_out, double *kmax_out)
 {
@@ -365,7 +365,11 @@ int ora_run(const ora_params *p, const void *dens, const void *xhii, int is_doub
     ora_forward(N, p->which_field, dens, xhii, is_double, p->use_only_phase, dk);
     const double L = (double)(float)p->box_size; /* grid.h:9 stores box_size as float */
     int written = 0;
-    for (int i = 0; i < nval && i < max_cfg; i++) { /* run.c:56-107 */
+    /* configurations [first, first + max_cfg) of the list; each one's ranges are
+       set afresh inside the loop (run.c:56-84), so skipping earlier ones changes
+       nothing */
+    for (int i = first < 0 ? 0 : first; i < nval && written < max_cfg; i++) { /* run.c:56-107 */
+        const int o = written;
         kpoly[n - 1] = kl[i];
         if (n == 2) kpoly[0] = kl[i];
         if (n == 3) {
@@ -381,17 +385,17 @@ int ora_run(const ora_params *p, const void *dens, const void *xhii, int is_doub
                                     2. * kpoly[0] * kpoly[1] * cmax);
             }
         }
-        B_out[i] = ora_polyspectrum(N, dk, n, kpoly, kpmin, kpmax, p->kbinwidth, p->kbinning, L,
+        B_out[o] = ora_polyspectrum(N, dk, n, kpoly, kpmin, kpmax, p->kbinwidth, p->kbinning, L,
                                     NULL, NULL);
-        npoly_out[i] = p->write_numpolygons == 1
+        npoly_out[o] = p->write_numpolygons == 1
                            ? ora_num_polygons(N, n, kpoly, kpmin, kpmax, p->kbinwidth, p->kbinning, L)
                            : 0.;
-        k_out[i] = kl[i];
-        theta_out[i] = th ? (p->equilateral == 1 ? th[0] : th[i]) : NAN;
+        k_out[o] = kl[i];
+        theta_out[o] = th ? (p->equilateral == 1 ? th[0] : th[i]) : NAN;
         for (int j = 0; j < n; j++) {
-            kpoly_out[i * n + j] = kpoly[j];
-            kmin_out[i * n + j] = kpmin[j];
-            kmax_out[i * n + j] = kpmax[j];
+            kpoly_out[o * n + j] = kpoly[j];
+            kmin_out[o * n + j] = kpmin[j];
+            kmax_out[o * n + j] = kpmax[j];
         }
         written++;
     }

@@ -78,12 +78,13 @@ int ora_num_configs(const ora_params *p);
 
 /* The run.c:29-107 loop: forward transform, then for each configuration the
  * kpolygon bookkeeping of run.c:56-84, polyspectrum() and num_polygons().
+ * Runs configurations [first, first + max_cfg) of the run's list.
  * Outputs (length max_cfg, or max_cfg*n for the per-leg arrays):
  *   k_out, theta_out (NaN where the run has no theta), B_out, npoly_out,
  *   kpoly_out / kmin_out / kmax_out: the kpolygon arrays after each config.
  * Returns the number of configurations written, <0 on error. */
 int ora_run(const ora_params *p, const void *dens, const void *xhii, int is_double,
-            int max_cfg, double *k_out, double *theta_out, double *B_out, double *npoly_out,
+            int first, int max_cfg, double *k_out, double *theta_out, double *B_out, double *npoly_out,
             double *kpoly_out, double *kmin_out, double *kmax_out);
 
 #ifdef __cplusplus

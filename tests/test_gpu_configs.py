@@ -5,8 +5,8 @@ stated shapes, spectra and seeds):
     values and the power spectrum over all shells, FP64 plain against the
     oracle (the reference's algorithm on the CPU), batched against both;
   * 256^3 XHII (4000 spheres, seed 2), L = 300: k1 = 0.5, k2 = 1.0, 20 theta
-    bins, GIVEN binning, cosThetaBinwidth 0.1; batched FP32 against plain FP64,
-    the first configurations also against the oracle;
+    bins, GIVEN binning, cosThetaBinwidth 0.1; all 20 bins against the oracle,
+    plain FP64 and batched FP32 (1e-5 relative, no absolute floor);
   * 1024^3 DENS lognormal (P ~ k^-1.5, seed 8), L = 1000: power spectrum over
     all 512 shells plus 128 triangle configurations (64 equilateral, 64
     isosceles k1 = k2 = 0.3); batched FP32 against plain FP64 on a sample of
@@ -53,6 +53,10 @@ def test_config_128_equilateral_and_power(gpu_lib, ora):
 
 
 def test_config_256_xhii_given(gpu_lib, ora):
+    """All 20 theta bins against the oracle: plain FP64 to 1e-9, batched FP32
+    to 1e-5 relative with no absolute floor (each bin's condition number is
+    computed too, so a bin near a zero crossing would show why), counts
+    exact, the k lists identical."""
     ps = gpu_lib
     n, box = 256, 300.0
     xhii = synth.ionised_spheres(n, box, 4000, 2)
@@ -61,18 +65,19 @@ def test_config_256_xhii_given(gpu_lib, ora):
         cfgs, k, th = ps.read_params_to_kvectors(n, box, 3, k1=0.5, k2=1.0, num_values=20,
                                                  kbinningCase=ps.PS_BIN_GIVEN, dcosTheta=0.1)
         B64, N64, _, _ = ctx.batch(cfgs, ps.PS_FP64_PLAIN)
-        B32, N32, _, _ = ctx.batch(cfgs, ps.PS_FP32_BATCHED)
+        B32, N32, kap, _ = ctx.batch(cfgs, ps.PS_FP32_BATCHED, kappa=True)
     assert len(B32) == 20
-    has = np.rint(N64) != 0
-    ok, _ = _close(B32[has], B64[has], 1e-5, 1e-6)
-    assert ok, (B32, B64)
-    np.testing.assert_array_equal(N32, np.rint(N64))
     p = ora.RunParams(grid_size=n, box_size=box, which_field=1, use_only_phase=0, n=3, equilateral=0, k1=0.5,
                       k2=1.0, num_values=20, kbinwidth=1.0, kbinning=2, dcos_theta=0.1)
-    ref = ora.ora_run(p, None, xhii, max_cfg=2)
-    np.testing.assert_array_equal(k[:2], ref.k)
-    assert np.all(np.abs(B64[:2] - ref.B) <= 1e-9 * np.abs(ref.B))
-    np.testing.assert_array_equal(N32[:2], np.rint(ref.npoly))
+    ref = ora.ora_run(p, None, xhii)
+    assert len(ref.B) == 20
+    np.testing.assert_array_equal(k, ref.k)
+    np.testing.assert_array_equal(N32, np.rint(ref.npoly))
+    assert np.all(np.rint(ref.npoly) > 0)
+    rel64 = np.abs(B64 - ref.B) / np.abs(ref.B)
+    rel32 = np.abs(B32 - ref.B) / np.abs(ref.B)
+    assert rel64.max() <= 1e-9, rel64
+    assert rel32.max() <= 1e-5, (rel32, kap)
 
 
 def _torch_lognormal(n, alpha, seed):
