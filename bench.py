@@ -50,10 +50,14 @@ def make_inputs(w):
     return dens, xhii
 
 
-def make_cfgs(ps, w):
+def make_cfgs(ps, w, copies: int = 1):
+    """The workload's configurations; with copies > 1 the four sweeps again
+    per copy r, both legs shifted by -0.005 r h/Mpc (distinct shells of about
+    the same cost: the multi-GPU workload of 64 configurations per rank)."""
     import ctypes as C
     allc = []
-    for k1, k2 in w["pairs"]:
+    pairs = [(k1 - 0.005 * r, k2 - 0.005 * r) for r in range(copies) for k1, k2 in w["pairs"]]
+    for k1, k2 in pairs:
         cfgs, _, _ = ps.read_params_to_kvectors(w["grid"], w["box"], 3, k1=k1, k2=k2,
                                                 num_values=w["num_values"],
                                                 kbinningCase=ps.PS_BIN_DERIVED)
@@ -147,25 +151,38 @@ def gpu_index(local_rank: int) -> str:
 
 
 # --------------------------------------------------------------------------- CPU
-def cpu_reference_sample(w, dens, xhii, first: int = 0, count: int = 1):
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_reference_sample(w, dens, xhii, first: int = 0, count: int = 1, threads: int | None = None):
     """Time the reference's CPU implementation on `count` configurations of the
     workload.  Uses oracle/_ref (the reference's own C, FFT shim) when built,
-    else the oracle restatement.  Returns (configs/s, kind, cores, sample, seconds)."""
+    else the oracle restatement.  `threads`: threads of the shim FFT (default:
+    every CPU).  Returns (configs/s, kind, cores, sample, seconds, RunResult)."""
     import oracle
     k1, k2 = w["pairs"][0]
     p = oracle.RunParams(grid_size=w["grid"], box_size=w["box"], which_field=2,
                          use_only_phase=w["use_only_phase"], n=3, equilateral=0, k1=k1, k2=k2,
                          num_values=w["num_values"], kbinning=1, kbinwidth=w["kbinwidth"])
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("PS_SHIM_THREADS", str(cores))
+    cores = threads or os.cpu_count() or 1
     t0 = time.time()
     if oracle.ref_available():
+        oracle.ref_set_threads(cores)
         r = oracle.ref_run(p, dens, xhii, first=first, count=count)
         kind = "reference"
         t_fwd, t_cfg = r.t_forward, r.t_configs
     else:
+        oracle.ora_set_threads(cores)
         t_a = time.time()
-        r = oracle.ora_run(p, dens, xhii, max_cfg=count)
+        r = oracle.ora_run(p, dens, xhii, max_cfg=count, first=first)
         kind = "port"
         t_cfg = time.time() - t_a
         t_fwd = 0.0
@@ -173,10 +190,10 @@ def cpu_reference_sample(w, dens, xhii, first: int = 0, count: int = 1):
     per_cfg = t_cfg / max(count, 1) + t_fwd / 64.0
     sample = (f"{count} of the 64 configurations (k1,k2)={w['pairs'][0]}, theta index {first}"
               f"{'..' + str(first + count - 1) if count > 1 else ''}, at {w['grid']}^3 plus the forward "
-              f"transform amortised over 64; reference C + FFT shim (FFTW not installed), shim FFT on "
-              f"{cores} threads, estimator loops single-threaded as in the reference; "
-              f"t_forward={t_fwd:.2f}s t_configs={t_cfg:.2f}s")
-    return 1.0 / per_cfg, kind, cores, sample, wall
+              f"transform amortised over 64; reference C + FFT shim (FFTW not installed; the shim stands "
+              f"in for FFTW), shim FFT on {cores} thread{'s' if cores > 1 else ''}, estimator loops "
+              f"single-threaded as in the reference; t_forward={t_fwd:.2f}s t_configs={t_cfg:.2f}s")
+    return 1.0 / per_cfg, kind, cores, sample, wall, r
 
 
 def run_reference(args, rank, world):
@@ -192,7 +209,7 @@ def run_reference(args, rank, world):
     info = None
     t_all = time.time()
     for s in range(steps):
-        v, kind, cores, sample, wall = cpu_reference_sample(w, dens, xhii, first=s, count=1)
+        v, kind, cores, sample, wall, _ = cpu_reference_sample(w, dens, xhii, first=s, count=1)
         vals.append(1.0 / v)
         info = (kind, cores, sample)
     per_cfg = float(np.mean(vals))
@@ -223,7 +240,19 @@ def run_ours(args, rank, world, local_rank):
     w = workload(args.grid)
     dens_np, xhii_np = make_inputs(w)
     N, box = w["grid"], w["box"]
-    cfgs = make_cfgs(ps, w)
+    sharded = world > 1 and not args.replicas
+    if sharded:
+        # weak scaling of the sharded path: 64 configurations per rank, whole
+        # sweeps partitioned over the ranks, one all-gather of results per step
+        from polyspectrum_b200 import multi
+        all_cfgs = make_cfgs(ps, w, copies=world)
+        parts = multi.partition(all_cfgs, world)
+        cfgs = multi.share(all_cfgs, parts[rank])
+        ncfg_total = len(all_cfgs)
+        share_max = max(len(p) for p in parts)
+    else:
+        cfgs = make_cfgs(ps, w)
+        ncfg_total = world * len(cfgs)
     ncfg = len(cfgs)
 
     # one non-default stream for torch and the library, so the timing events
@@ -250,9 +279,22 @@ def run_ours(args, rank, world, local_rank):
     spectrum_band = plan.band if not args.full_spectrum else -1
     ctx.set_spectrum_band(spectrum_band)
 
+    if sharded:
+        resbuf = torch.zeros(8 * share_max, dtype=torch.float64, device=dev)
+        gathered = torch.zeros(world * 8 * share_max, dtype=torch.float64, device=dev)
+
+    def exchange():
+        """The step's result exchange (sharded runs): this rank's results
+        copied on the device, one NCCL all-gather over the ranks."""
+        if sharded:
+            plan.results_to_device(resbuf.data_ptr())
+            dist.all_gather_into_tensor(gathered, resbuf)
+
     def step():
         ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
-        return plan.execute()
+        r = plan.execute()
+        exchange()
+        return r
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
@@ -268,6 +310,7 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(k):
             ctx.set_field_async(ps.PS_FIELD_XHI_DENS, a, b, use_only_phase=1)
             plan.launch()
+            exchange()
         e1.record(stream)
         torch.cuda.synchronize()
         ctx.synchronize()
@@ -280,6 +323,7 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(k):
             ctx.set_field_async(ps.PS_FIELD_XHI_DENS, a, b, use_only_phase=1)
             subs.append(plan.submit())
+            exchange()
         ctx.synchronize()
         return subs
 
@@ -315,7 +359,7 @@ def run_ours(args, rank, world, local_rank):
     t_clk1 = time.time()
     timed_launches = ctx.launch_count() - n_launch0
     ms_step = ms / args.steps
-    value = world * ncfg / (ms_step / 1e3)
+    value = ncfg_total / (ms_step / 1e3)
     Bl, Nl, _, _ = plan.results()
     assert np.array_equal(Bl, B32) and np.array_equal(Nl, N32)
 
@@ -324,7 +368,7 @@ def run_ours(args, rank, world, local_rank):
     if spectrum_band >= 0:
         ctx.set_spectrum_band(-1)
         steps_queued(2, dens, xhii)
-        value_full = world * ncfg / (timed_device(args.steps, dens, xhii) / args.steps / 1e3)
+        value_full = ncfg_total / (timed_device(args.steps, dens, xhii) / args.steps / 1e3)
         Bl, Nl, _, _ = plan.results()
         assert np.array_equal(Bl, B32) and np.array_equal(Nl, N32)
         ctx.set_spectrum_band(spectrum_band)
@@ -364,9 +408,19 @@ def run_ours(args, rank, world, local_rank):
                                GBps=(s["bytes"] / (s["ms"] / 1e3) / 1e9) if s["ms"] > 0 and s["bytes"] > 0 else None)
                for s in stats}
 
+    # ---- condition numbers of the configurations (one eager execution with
+    # the |term| sums; the error of each B is about kappa * 2^-24)
+    kplan = ctx.plan(cfgs, method=ps.PS_FP32_BATCHED, graph=False, kappa=True)
+    ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+    _, _, kappa, cfg_out = kplan.execute()
+    kplan.close()
+    kmin32 = np.array([[cfg_out[q].kmin[j] for j in range(3)] for q in range(ncfg)])
+    kmax32 = np.array([[cfg_out[q].kmax[j] for j in range(3)] for q in range(ncfg)])
+
     # ---- end to end: pinned host inputs, copies and result read-back inside.
     # Pipelined (the API's asynchronous calls): the upload of step k+1 runs on
-    # the copy engine while step k's configurations run.  Serial: blocking calls.
+    # the copy engine while step k's configurations run.  Serial: blocking
+    # calls.  Each mode is timed three times, alternating.
     dens_h = torch.from_numpy(dens_np).pin_memory()
     xhii_h = torch.from_numpy(xhii_np).pin_memory()
 
@@ -389,32 +443,46 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(args.steps):
             ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens_h, xhii_h, use_only_phase=1)
             plan.execute()
+            exchange()
+
+    load_stats = []
+
+    def pipelined():
+        steps_queued(args.steps, dens_h, xhii_h)
+        load_stats.append(ctx.load_stats())
 
     steps_queued(2, dens_h, xhii_h)
-    ms_e2e = timed_host(lambda: steps_queued(args.steps, dens_h, xhii_h))
-    e2e_value = world * ncfg / (ms_e2e / args.steps / 1e3)
-    ms_e2e_serial = timed_host(serial)
+    ms_pipe, ms_serial = [], []
+    for _ in range(3):
+        ms_pipe.append(timed_host(pipelined) / args.steps)
+        ms_serial.append(timed_host(serial) / args.steps)
+    ms_e2e = float(np.median(ms_pipe))
+    e2e_value = ncfg_total / (ms_e2e / 1e3)
+    ms_e2e_serial = float(np.median(ms_serial))
     time.sleep(0.1)
     clk = clocks.summary(windows)  # the device-timed and the end-to-end timed regions
     clocks.close()
     h2d = ctx.upload_bytes()  # the library composes dens*(1-xHII) on the host: one float grid per step
     d2h = ncfg * 8 * 8 + 4  # per configuration B, Npoly, 6 derived k bounds; one status word
+    ls = load_stats[-1]
+    host_load = dict(rows=ls["rows"], rows_raw=ls["rows_raw"], raw_frac=ls["rows_raw"] / max(ls["rows"], 1),
+                     compose_ms=ls["compose_s"] * 1e3, raw_copy_ms=ls["raw_copy_ms"],
+                     host_threads=ls["host_threads"], cpus=os.cpu_count(),
+                     note="last load of the last pipelined repeat: rows sent raw (dens and xHII) vs composed "
+                          "on host threads (one float per cell), host compose time and raw-row copy time")
 
-    # ---- plain FP64 method on a sample of the same configurations (rank 0)
+    # ---- plain FP64 method on all 64 configurations (rank 0): the metric's
+    # denominator and the error of every batched B against it
     plain = None
-    if rank == 0 and not args.no_plain:
+    parity = None
+    if rank == 0 and world == 1 and not args.no_plain:
         plan.close()
         ctx.close()
         torch.cuda.empty_cache()
-        sel = [0, 16, 32, 48] if ncfg >= 49 else list(range(min(4, ncfg)))
-        import ctypes as C
-        sub = (ps.ps_cfg * len(sel))()
-        for i, q in enumerate(sel):
-            C.memmove(C.byref(sub[i]), C.byref(cfgs[q]), C.sizeof(ps.ps_cfg))
         with ps.Context(N, box, methods=ps.PS_FP64_PLAIN, device=local_rank) as c64:
             c64.set_stream(stream.cuda_stream)
             c64.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
-            c64.batch(sub[:1], ps.PS_FP64_PLAIN)
+            c64.batch(cfgs[:1], ps.PS_FP64_PLAIN)
             torch.cuda.synchronize()
             e0.record(stream)
             c64.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
@@ -422,23 +490,57 @@ def run_ours(args, rank, world, local_rank):
             torch.cuda.synchronize()
             t_fwd64 = e0.elapsed_time(e1)
             e0.record(stream)
-            B64, N64, _, _ = c64.batch(sub, ps.PS_FP64_PLAIN)
+            B64, N64, _, out64 = c64.batch(cfgs, ps.PS_FP64_PLAIN)
             e1.record(stream)
             torch.cuda.synchronize()
-            t_cfg64 = e0.elapsed_time(e1) / len(sel)
+            t_cfg64 = e0.elapsed_time(e1) / ncfg
         per_cfg64 = t_cfg64 + t_fwd64 / ncfg
-        b32 = B32[sel]
-        rel = np.abs(b32 - B64) / np.abs(B64)
+        rel = np.abs(B32 - B64) / np.abs(B64)
+        kmin64 = np.array([[out64[q].kmin[j] for j in range(3)] for q in range(ncfg)])
+        kmax64 = np.array([[out64[q].kmax[j] for j in range(3)] for q in range(ncfg)])
         plain = dict(configs_per_s=1e3 / per_cfg64, ms_per_config=t_cfg64, forward_ms=t_fwd64,
-                     sample=f"configurations {sel} of the sweep",
+                     sample=f"all {ncfg} configurations of the sweep",
                      batched_vs_plain_speedup=value / world / (1e3 / per_cfg64),
                      max_rel_err_B_fp32_vs_fp64=float(rel.max()),
-                     counts_equal=bool(np.array_equal(N32[sel], np.rint(N64))))
+                     counts_equal=bool(np.array_equal(N32, np.rint(N64))))
+        eps32 = 2.0 ** -24
+        parity = dict(
+            tolerance="|dB| <= 1e-5 |B| per configuration (no absolute floor); counts exact; DERIVED k-ranges "
+                      "bit-identical",
+            fp64_plain=dict(configs=ncfg, max_rel_err_B=float(rel.max()), median_rel_err_B=float(np.median(rel)),
+                            within_1e_5=bool((rel <= 1e-5).all()),
+                            counts_equal=bool(np.array_equal(N32, np.rint(N64))),
+                            derived_equal=bool(np.array_equal(kmin32, kmin64) and np.array_equal(kmax32, kmax64))),
+            kappa=dict(max=float(np.max(kappa)), median=float(np.median(kappa)),
+                       at_max_rel_err=float(kappa[int(np.argmax(rel))]),
+                       max_rel_err_over_kappa_eps32=float(np.max(rel / (kappa * eps32)))))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, kind, cores, sample, wall = cpu_reference_sample(w, dens_np, xhii_np)
-        cpu = dict(value=v, unit=UNIT, cores=cores, kind=kind, sample=sample)
+        # the reference itself on configuration 0 of the sweep ((k1,k2) = (0.2,0.5),
+        # theta index 0) at 512^3, all host threads; its result checks the GPU's
+        v, kind, cores, sample, wall, r = cpu_reference_sample(w, dens_np, xhii_np)
+        cpu = dict(value=v, unit=UNIT, cores=cores, kind=kind, sample=sample, nproc=os.cpu_count(),
+                   cpu_model=cpu_model(),
+                   note="the reference's C with this repository's FP64 FFT shim standing in for FFTW (not "
+                        "installed); the reference's MPI path is unavailable on this box (no MPI / FFTW-MPI)")
+        if parity is not None:
+            rel0 = abs(B32[0] - r.B[0]) / abs(r.B[0])
+            parity["reference"] = dict(
+                config="(k1,k2)=(0.2,0.5) h/Mpc, theta index 0, 512^3 (pair group on the 128-point sub-grid)",
+                kind=kind, B_reference=float(r.B[0]), B_gpu=float(B32[0]), rel_err_B=float(rel0),
+                within_1e_5=bool(rel0 <= 1e-5), npoly_reference=float(r.npoly[0]), npoly_gpu=float(N32[0]),
+                npoly_equal=bool(N32[0] == np.rint(r.npoly[0])),
+                derived_equal=bool(np.array_equal(kmin32[0], r.kmin[0]) and np.array_equal(kmax32[0], r.kmax[0])))
+        if not args.no_serial_cpu:
+            # one thread (the reference's serial path) at sizes where that is cheap
+            serial_runs = []
+            for g in (128, 256):
+                ws = workload(g)
+                ds, xs = make_inputs(ws)
+                vs, kind_s, _, sample_s, _, _ = cpu_reference_sample(ws, ds, xs, threads=1)
+                serial_runs.append(dict(grid=g, value=vs, unit=UNIT, cores=1, kind=kind_s, sample=sample_s))
+            cpu["serial_1_thread"] = serial_runs
 
     if rank == 0:
         out = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
@@ -449,21 +551,30 @@ def run_ours(args, rank, world, local_rank):
                                theta_bins=w["num_values"], configs_per_step=ncfg,
                                binning="DERIVED", kbinwidth=1.0, use_only_phase=1,
                                l2="inputs (2 x 512 MiB) and every pass larger than L2; no flush",
-                               parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                               parallelism=("single GPU" if world == 1 else
+                                            f"replicas x{world}" if not sharded else
+                                            f"sharded over {world} ranks: {ncfg_total} configurations "
+                                            f"(64 per rank, whole sweeps per rank), one NCCL all-gather "
+                                            f"of the results per step"),
+                               configs_total=ncfg_total,
                                subgrids=[int(ln.split()[-1]) for ln in tune_table.splitlines() if ln.startswith("grid")],
                                spectrum_band=spectrum_band, value_full_spectrum=value_full),
                    e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d,
-                            d2h_bytes_per_step=d2h, ms_per_step=ms_e2e / args.steps,
+                            d2h_bytes_per_step=d2h, ms_per_step=ms_e2e,
+                            ms_per_step_repeats=ms_pipe,
                             mode="pipelined: ps_gpu_set_field_async + ps_gpu_plan_submit per step, "
                                  "one ps_gpu_synchronize after the last; the library composes "
                                  "dens*(1-xHII) of the two host grids on host threads and uploads one",
-                            serial_value=world * ncfg / (ms_e2e_serial / args.steps / 1e3),
-                            serial_ms_per_step=ms_e2e_serial / args.steps,
-                            serial_mode="ps_gpu_set_field + ps_gpu_plan_execute per step (blocking)"),
+                            serial_value=ncfg_total / (ms_e2e_serial / 1e3),
+                            serial_ms_per_step=ms_e2e_serial, serial_ms_per_step_repeats=ms_serial,
+                            serial_mode="ps_gpu_set_field + ps_gpu_plan_execute per step (blocking)",
+                            host_load=host_load),
                    gpu_launches=timed_launches, roofline=roof,
                    whole_step=dict(alg_bytes=all_alg / args.steps,
-                                   achieved_GBps=all_alg / args.steps / (ms_step / 1e3) / 1e9),
-                   kernels=kernels, clocks=clk, plain_fp64=plain, cpu_baseline=cpu)
+                                   achieved_GBps=all_alg / args.steps / (ms_step / 1e3) / 1e9,
+                                   frac=all_alg / args.steps / (ms_step / 1e3) / 1e9 / peak,
+                                   peak=peak, peak_source=peak_kind),
+                   kernels=kernels, clocks=clk, plain_fp64=plain, parity=parity, cpu_baseline=cpu)
         print(json.dumps(out), flush=True)
 
 
@@ -476,6 +587,11 @@ def main():
     ap.add_argument("--grid", type=int, default=512, help="grid size (the workload is 512)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-serial-cpu", action="store_true",
+                    help="skip the 1-thread reference runs at 128^3 and 256^3")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with --gpus N > 1: N independent replicas of the 64-configuration step instead of the "
+                         "sharded path")
     ap.add_argument("--full-spectrum", action="store_true",
                     help="transform the field up to Nyquist instead of the plan's band")
     ap.add_argument("--no-autotune", action="store_true",

@@ -178,9 +178,12 @@ void ps_gpu_plan_destroy(ps_gpu_plan *plan);
  * ps_gpu_set_field without waiting: host arrays are copied on the context's
  * copy stream into one of two device staging slots, and the forward transform
  * is queued on the compute stream behind that copy.  ps_gpu_plan_submit queues
- * a PS_FP32_BATCHED plan execution behind it; its results reach B, Npoly (and
- * kappa, cfgs_out) in stream order, by a host callback.  So the upload of
- * field k+1 overlaps the configurations of field k.  Every pointer passed to
+ * a PS_FP32_BATCHED plan execution behind it and the copy of its results to
+ * a page-locked buffer of its own; they are unpacked into B, Npoly (and kappa,
+ * cfgs_out) by the first later call on the context (ps_gpu_set_field_async,
+ * ps_gpu_plan_submit, ps_gpu_synchronize) that finds the copy done, at the
+ * latest by ps_gpu_synchronize; no host callback holds the streams.  So the
+ * upload of field k+1 overlaps the configurations of field k.  Every pointer passed to
  * these two calls (inputs and outputs) must stay valid and the inputs
  * unchanged until ps_gpu_synchronize returns; host inputs overlap only when
  * they are page-locked (cudaHostAlloc / cudaHostRegister).  Errors detected on
@@ -197,6 +200,19 @@ int ps_gpu_set_field_async(ps_gpu_ctx *ctx, int which, const void *dens, const v
  * two-array upload.  ps_gpu_upload_bytes gives the host -> device bytes of
  * the last host field load (no reference counterpart). */
 long long ps_gpu_upload_bytes(const ps_gpu_ctx *ctx);
+/* Statistics of the last host field load: rows (N^2) and rows sent as they
+ * are (rows_raw; the others were composed on host threads), host seconds
+ * spent composing, device milliseconds of the raw rows' copies, the raw
+ * fraction the next load will use, the host threads of the composition
+ * ($PS_HOST_THREADS, default: the CPUs this process may run on less one; one
+ * pool per process) and the host -> device bytes.  Zeros for loads that
+ * compose nothing (device inputs, other fields).  No reference counterpart. */
+typedef struct {
+    long long rows, rows_raw, bytes;
+    double compose_s, raw_copy_ms, next_raw_frac;
+    int host_threads;
+} ps_load_stats;
+int ps_gpu_load_stats(const ps_gpu_ctx *ctx, ps_load_stats *out);
 int ps_gpu_plan_submit(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
                        double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
 int ps_gpu_synchronize(ps_gpu_ctx *ctx);
@@ -209,6 +225,13 @@ int ps_gpu_synchronize(ps_gpu_ctx *ctx);
 int ps_gpu_plan_launch(ps_gpu_ctx *ctx, ps_gpu_plan *plan);
 int ps_gpu_plan_results(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
                         double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
+/* Queues, on the context's stream, a copy of the latest execution's results
+ * into device memory dst (8 * nconf doubles): B and Npoly interleaved per
+ * configuration (2 * nconf), then the DERIVED k-ranges, six per configuration
+ * (kmin, kmax of legs 0, 1, 2; zeros for other binnings).  No wait: for an
+ * exchange that stays on the device (an all-gather over ranks, the
+ * counterpart of the reference's MPI reduction, polyspectrum.c:144-153). */
+int ps_gpu_plan_results_device(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *dst);
 
 /* The context's autotuned choices as text, one "grid N b_a b_b b_c M" line per
  * pair-group signature: writes at most buflen bytes (NUL-terminated) and
@@ -227,7 +250,11 @@ long long ps_gpu_launch_count(ps_gpu_ctx *ctx);
  * (out_is_double = 0) or double (1) in host or device memory (out_mem).  No
  * reference counterpart.  For a phase-only field (use_only_phase = 1) the
  * gradient goes through z/|z| and needs the modulus kept at loading
- * (ps_gpu_keep_modulus); without it PS_ERR_UNSUPPORTED. */
+ * (ps_gpu_keep_modulus); without it PS_ERR_UNSUPPORTED.  The normalisation
+ * needs the configuration's polygon count: when an earlier
+ * ps_gpu_polyspectrum(_batch) call on this context evaluated the same
+ * configuration with the same method, its count is reused (counts depend on
+ * the shells only), else the call evaluates the configuration first. */
 int ps_gpu_grad(ps_gpu_ctx *ctx, int method, int n, const double *k, const double *kmin,
                 const double *kmax, double kbinwidth, int kbinningCase, void *out,
                 int out_is_double, int out_mem);
@@ -302,6 +329,16 @@ int ps_gpu_kernel_stats(ps_gpu_ctx *ctx, ps_kernel_stat *out, int max);
 int ps_gpu_power_spectrum_noalloc(int nbins, double boxsize, const float *field_dev,
                                   int use_only_phase, int nshell, const double *k,
                                   double kbinwidth, double *P, double *Npoly, void *stream);
+
+/* Host-side fault injection for tests of the error paths (no reference
+ * counterpart; the reference exit()s on these failures, grid.c:24,133,
+ * utils.c:96).  spec "alloc:N", "read:N" or "launch:N" (comma-separated to arm
+ * several): the Nth device or page-locked allocation, input-file read or
+ * post-launch status check after this call fails once, with the status a
+ * real failure returns (PS_ERR_OOM, PS_ERR_IO, PS_ERR_CUDA); no GPU fault is
+ * caused.  NULL or "" disarms.  $PS_FAULT arms the same way at the process's
+ * first ps_gpu_create.  Malformed spec: PS_ERR_ARG. */
+int ps_gpu_debug_fault(const char *spec);
 
 void ps_gpu_finalize(ps_gpu_ctx *ctx);
 const char *ps_gpu_strerror(int status);

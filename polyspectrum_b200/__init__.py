@@ -58,6 +58,12 @@ class ps_kernel_stat(C.Structure):
                 ("bytes", C.c_double)]
 
 
+class ps_load_stats(C.Structure):
+    _fields_ = [("rows", C.c_longlong), ("rows_raw", C.c_longlong), ("bytes", C.c_longlong),
+                ("compose_s", C.c_double), ("raw_copy_ms", C.c_double), ("next_raw_frac", C.c_double),
+                ("host_threads", C.c_int)]
+
+
 _lib = None
 
 
@@ -85,6 +91,9 @@ def lib() -> C.CDLL:
     L.ps_gpu_plan_destroy.restype = None
     L.ps_gpu_set_field_async.argtypes = [vp, ip, vp, vp, ip, ip, ip]
     L.ps_gpu_set_field_files.argtypes = [vp, ip, C.c_char_p, ip, C.c_char_p, ip, ip]
+    L.ps_gpu_load_stats.argtypes = [vp, C.POINTER(ps_load_stats)]
+    L.ps_gpu_debug_fault.argtypes = [C.c_char_p]
+    L.ps_gpu_plan_results_device.argtypes = [vp, vp, vp]
     L.ps_gpu_upload_bytes.argtypes = [vp]
     L.ps_gpu_upload_bytes.restype = C.c_longlong
     L.ps_gpu_plan_submit.argtypes = [vp, vp, dp, dp, dp, C.POINTER(ps_cfg)]
@@ -113,10 +122,17 @@ def lib() -> C.CDLL:
                  "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize",
                  "ps_gpu_tune_export", "ps_gpu_tune_import", "ps_gpu_keep_modulus",
                  "ps_gpu_set_spectrum_band", "ps_gpu_plan_band", "ps_gpu_plan_launch", "ps_gpu_plan_results",
-                 "ps_gpu_set_field_files"):
+                 "ps_gpu_set_field_files", "ps_gpu_load_stats", "ps_gpu_debug_fault",
+                 "ps_gpu_plan_results_device"):
         getattr(L, name).restype = ip
     _lib = L
     return L
+
+
+def debug_fault(spec: str | None) -> None:
+    """Arm host-side fault injection ("alloc:N", "read:N", "launch:N"; None
+    disarms): see ps_gpu_debug_fault."""
+    _check(lib().ps_gpu_debug_fault(None if spec is None else spec.encode()))
 
 
 def _check(status: int) -> int:
@@ -252,6 +268,12 @@ class Context:
         """Host -> device bytes of the last host field load (ps_gpu_upload_bytes)."""
         return int(lib().ps_gpu_upload_bytes(self._h))
 
+    def load_stats(self) -> dict:
+        """Statistics of the last host field load (ps_gpu_load_stats)."""
+        st = ps_load_stats()
+        _check(lib().ps_gpu_load_stats(self._h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in ps_load_stats._fields_}
+
     def launch_count(self) -> int:
         """Kernels executed by this context since its creation."""
         return int(lib().ps_gpu_launch_count(self._h))
@@ -386,6 +408,11 @@ class Plan:
         _check(lib().ps_gpu_plan_results(self.ctx.handle, self._h, _dptr(B), _dptr(Np),
                                          _dptr(kap) if self.kappa else None, out))
         return B, Np, kap, out
+
+    def results_to_device(self, dst_ptr: int):
+        """Queue a copy of the latest execution's results into device memory
+        (8 doubles per configuration, ps_gpu_plan_results_device)."""
+        _check(lib().ps_gpu_plan_results_device(self.ctx.handle, self._h, C.c_void_p(dst_ptr)))
 
     def submit(self) -> "Submission":
         """Queue one execution on the field most recently loaded (ps_gpu_plan_submit);

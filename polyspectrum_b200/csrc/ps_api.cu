@@ -45,6 +45,64 @@ int fail(int code, const char* fmt, ...)
     va_end(ap);
     return code;
 }
+// Host-side fault injection, for tests of the error paths (no GPU fault is
+// ever caused): once armed with "alloc:N", "read:N" or "launch:N" (a comma
+// separated list arms several), the Nth device or page-locked allocation,
+// input-file read or post-launch status check after arming fails once, with
+// the status the real failure returns (PS_ERR_OOM, PS_ERR_IO, PS_ERR_CUDA).
+// Armed by ps_gpu_debug_fault, or by $PS_FAULT at the first ps_gpu_create.
+enum FaultKind { FAULT_ALLOC = 0, FAULT_READ = 1, FAULT_LAUNCH = 2, FAULT_KINDS = 3 };
+std::atomic<long long> g_fault_at[FAULT_KINDS];
+std::atomic<long long> g_fault_seen[FAULT_KINDS];
+
+bool fault_hit(int kind)
+{
+    const long long at = g_fault_at[kind].load();
+    if (at <= 0) return false;
+    if (++g_fault_seen[kind] != at) return false;
+    g_fault_at[kind] = 0;  // one shot
+    return true;
+}
+
+int arm_faults(const char* spec)
+{
+    long long at[FAULT_KINDS] = {0, 0, 0};
+    static const char* names[FAULT_KINDS] = {"alloc", "read", "launch"};
+    if (spec && *spec) {
+        std::string txt(spec);
+        size_t pos = 0;
+        while (pos <= txt.size()) {
+            size_t end = txt.find(',', pos);
+            if (end == std::string::npos) end = txt.size();
+            const std::string item = txt.substr(pos, end - pos);
+            const size_t colon = item.find(':');
+            int kind = -1;
+            for (int q = 0; q < FAULT_KINDS && colon != std::string::npos; q++)
+                if (item.compare(0, colon, names[q]) == 0 && colon == strlen(names[q])) kind = q;
+            char* tail = nullptr;
+            const long long n = kind >= 0 ? strtoll(item.c_str() + colon + 1, &tail, 10) : 0;
+            if (kind < 0 || n <= 0 || !tail || *tail) return fail(PS_ERR_ARG, "fault spec '%s': want alloc:N, read:N "
+                                                                               "or launch:N, N >= 1", item.c_str());
+            at[kind] = n;
+            pos = end + 1;
+        }
+    }
+    for (int q = 0; q < FAULT_KINDS; q++) {
+        g_fault_seen[q] = 0;
+        g_fault_at[q] = at[q];
+    }
+    return PS_OK;
+}
+
+// cudaGetLastError after launches, or the injected launch failure.
+cudaError_t launch_status()
+{
+    if (fault_hit(FAULT_LAUNCH)) {
+        cudaGetLastError();
+        return cudaErrorLaunchFailure;
+    }
+    return cudaGetLastError();
+}
 }  // namespace
 
 #define PS_CK(x)                                                                             \
@@ -98,22 +156,30 @@ template <typename T> struct PrecBufs {
     std::map<int, std::array<V2<T>*, 3>> sub;
 };
 
-// Host worker threads (one per CPU this process may run on, at most 64),
-// started once per context: run(f) calls f(t) on every worker t and returns
-// when all are done.
+// Host worker threads of the composition, one pool per process shared by
+// every context: $PS_HOST_THREADS threads, else one per CPU this process may
+// run on less one (left to the CUDA driver's threads and the caller), at most
+// 64.  run(f) calls f(t) on every worker t and returns when all are done; jobs
+// of different contexts (host threads) take turns.
 struct HostPool {
     std::vector<std::thread> th;
-    std::mutex m;
+    std::mutex m, turn;
     std::condition_variable cv, done_cv;
     std::function<void(size_t)> job;
     size_t gen = 0, pending = 0, n = 1;
     bool stop = false;
-    HostPool()
+    static size_t default_threads()
     {
+        const char* e = getenv("PS_HOST_THREADS");
+        if (e && atoi(e) > 0) return (size_t)std::min(atoi(e), 64);
         cpu_set_t set;
         CPU_ZERO(&set);
         const int ncpu = sched_getaffinity(0, sizeof(set), &set) == 0 ? CPU_COUNT(&set) : 1;
-        n = (size_t)std::max(1, std::min(ncpu, 64));
+        return (size_t)std::max(1, std::min(ncpu - 1, 64));
+    }
+    HostPool()
+    {
+        n = default_threads();
         for (size_t t = 1; t < n; t++)
             th.emplace_back([this, t]() {
                 size_t seen = 0;
@@ -132,6 +198,7 @@ struct HostPool {
     }
     void run(const std::function<void(size_t)>& f)
     {
+        std::lock_guard<std::mutex> one_job(turn);
         {
             std::lock_guard<std::mutex> lk(m);
             job = f;
@@ -152,6 +219,26 @@ struct HostPool {
         cv.notify_all();
         for (auto& t : th) t.join();
     }
+    // the process's pool, started on first use (never destroyed: its threads
+    // sleep on a condition variable until the process exits)
+    static HostPool& get()
+    {
+        static HostPool* pool = new HostPool();
+        return *pool;
+    }
+};
+
+// A plan execution queued by ps_gpu_plan_submit whose results are still on
+// their way: the copy into `host` (page-locked, this submission's own) ends
+// with `done`; the next call on the context that finds the event complete
+// unpacks them into the caller's arrays.
+struct PendingSubmit {
+    const ps_gpu_plan* P;
+    double* host;
+    size_t host_len;
+    cudaEvent_t done;
+    double *B, *Np, *kappa;
+    ps_cfg* cfgs_out;
 };
 
 struct ps_gpu_ctx {
@@ -209,9 +296,19 @@ struct ps_gpu_ctx {
     // split of a host XHI_DENS load between raw rows (PCIe) and composed rows
     // (host threads): the raw fraction and the measured seconds per row
     double raw_frac = 0.3, t_comp_row = 0.0, t_up_row = 0.0;
-    HostPool* pool = nullptr;  // host threads of the composition, made on first use
+    // statistics of the last host XHI_DENS load (ps_gpu_load_stats)
+    long long load_rows = 0, load_rows_raw = 0;
+    double load_compose_s = 0.0, load_raw_copy_ms = 0.0;
+    // asynchronous submissions not yet unpacked, oldest first, and spare
+    // page-locked result buffers / events for the next ones
+    std::vector<PendingSubmit> pending;
+    std::vector<std::pair<double*, size_t>> spare_host;
+    std::vector<cudaEvent_t> spare_events;
+    // polygon counts of configurations evaluated on this context (field
+    // independent), keyed by method and configuration: ps_gpu_grad reuses them
+    std::map<std::string, double> npoly_cache;
     cudaEvent_t ev_raw[2] = {nullptr, nullptr};
-    std::atomic<int> async_err{0};  // status of work whose results arrived in a host callback
+    std::atomic<int> async_err{0};  // status of submissions unpacked after their call returned
     std::set<ps_gpu_plan*> plans;   // live plans (finalize releases their device memory)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
@@ -267,6 +364,7 @@ template <typename T> int pw(int N)
 template <typename T> int alloc_dev(T** p, size_t count)
 {
     if (*p) return PS_OK;
+    if (fault_hit(FAULT_ALLOC)) return fail(PS_ERR_OOM, "cudaMalloc of %zu bytes: injected failure", sizeof(T) * count);
     cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -591,7 +689,7 @@ int c2r_shell(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, T* out, co
         pf.end(fam<T>(KF_INV_Z), NN2 * hb * V + extra, N);
     }
     if (reduce) PS_TRY(sum_partials(c, nb, 1, dsum, 1));
-    PS_CK(cudaGetLastError());
+    PS_CK(launch_status());
     return PS_OK;
 }
 
@@ -697,7 +795,7 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
                                                          (2 * band + 1 < N ? 2 * band + 1 : N) * H * V, N);
     }
     c->loaded_band = band;
-    PS_CK(cudaGetLastError());
+    PS_CK(launch_status());
     B.have_spec = true;
     B.have_mod = mod != nullptr;
     return PS_OK;
@@ -750,7 +848,7 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
         }
         PS_TRY(didx ? sum_partials(c, nb, cnt, dout, 1, didx + s0) : sum_partials(c, nb, cnt, dout + s0, 1));
     }
-    PS_CK(cudaGetLastError());
+    PS_CK(launch_status());
     return PS_OK;
 }
 
@@ -836,7 +934,7 @@ int derive_ranges(ps_gpu_ctx* c, const std::vector<Shell>& sh, std::vector<doubl
         k_derived_range<<<blocks, 256, 0, c->stream>>>(N, c->dshells + s, hmax, c->dminmax + 2 * s);
         pf.end(KF_DERIVED, 0.0);
     }
-    PS_CK(cudaGetLastError());
+    PS_CK(launch_status());
     PS_CK(cudaMemcpyAsync(init.data(), c->dminmax, 16 * (size_t)ns, cudaMemcpyDeviceToHost, c->stream));
     PS_CK(cudaStreamSynchronize(c->stream));
     const double pi = ref_pi();
@@ -981,6 +1079,32 @@ int legs_band(const std::vector<Shell>& legs, int N)
     int b = 0;
     for (const Shell& sh : legs) b = std::max(b, std::min(sh.band, N / 2));
     return b;
+}
+
+// Key of a configuration's polygon count: the method and what selects the
+// shells (DERIVED ranges are outputs, not inputs).
+std::string npoly_key(int method, const ps_cfg& g)
+{
+    std::string k;
+    auto add = [&](double v) { k.append(reinterpret_cast<const char*>(&v), sizeof(v)); };
+    k.push_back((char)method);
+    k.push_back((char)g.n);
+    k.push_back((char)g.kbinningCase);
+    add(g.kbinwidth);
+    for (int l = 0; l < g.n && l < PS_MAX_LEGS; l++) {
+        add(g.k[l]);
+        if (g.kbinningCase != PS_BIN_DERIVED) {
+            add(g.kmin[l]);
+            add(g.kmax[l]);
+        }
+    }
+    return k;
+}
+
+void remember_npoly(ps_gpu_ctx* c, int method, int nconf, const ps_cfg* in, const double* Np)
+{
+    if (c->npoly_cache.size() + (size_t)nconf > 4096) c->npoly_cache.clear();
+    for (int q = 0; q < nconf; q++) c->npoly_cache[npoly_key(method, in[q])] = Np[q];
 }
 
 int plain_batch(ps_gpu_ctx* c, int nconf, ps_cfg* cfgs, double* B, double* Np, double* kappa)
@@ -1506,9 +1630,11 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
     PS_TRY(plan_alloc(P, &gD, gs));
     PS_TRY(plan_alloc(P, &P->dres, 2 * (size_t)nconf));
     PS_TRY(plan_alloc(P, &P->dwb, 6 * (size_t)nconf));
+    PS_CK(cudaMemset(P->dwb, 0, 48 * (size_t)nconf));  // entries of non-DERIVED configurations stay 0
     PS_TRY(plan_alloc(P, &P->derr, 1));
     PS_CK(cudaMemset(P->derr, 0, sizeof(int)));
-    if (cudaHostAlloc((void**)&P->hres, (10 * (size_t)nconf + 1) * sizeof(double), cudaHostAllocDefault) !=
+    if (fault_hit(FAULT_ALLOC) ||
+        cudaHostAlloc((void**)&P->hres, (10 * (size_t)nconf + 1) * sizeof(double), cudaHostAllocDefault) !=
         cudaSuccess) {
         P->hres = nullptr;
         return fail(PS_ERR_OOM, "pinned result buffer of %d configurations", nconf);
@@ -1738,7 +1864,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         Prof pf(c);
         k_finalize<<<(nconf + 127) / 128, 128, 0, c->stream>>>(nconf, dcoef, sumD, sumI, 1.0 / n3, 1, dres);
         pf.end(KF_FINAL, 0.0);
-        PS_CK(cudaGetLastError());
+        PS_CK(launch_status());
         return PS_OK;
     });
     return PS_OK;
@@ -1752,10 +1878,9 @@ int plan_enqueue(ps_gpu_ctx* c, ps_gpu_plan* P)
 
 // Results of an executed batched plan: device -> pinned host copy (stream
 // ordered), then unpacked on the host into the caller's arrays.
-int plan_copy_results(ps_gpu_ctx* c, ps_gpu_plan* P)
+int plan_copy_results(ps_gpu_ctx* c, ps_gpu_plan* P, double* h)
 {
     const size_t n = (size_t)P->nconf;
-    double* h = P->hres;
     PS_CK(cudaMemcpyAsync(h, P->dres, 16 * n, cudaMemcpyDeviceToHost, c->stream));
     PS_CK(cudaMemcpyAsync(h + 2 * n, P->dwb, 48 * n, cudaMemcpyDeviceToHost, c->stream));
     if (P->flags & PS_PLAN_KAPPA) {
@@ -1766,11 +1891,10 @@ int plan_copy_results(ps_gpu_ctx* c, ps_gpu_plan* P)
     return PS_OK;
 }
 
-// Host side of a finished execution (no CUDA calls: also runs as a stream callback).
-int plan_unpack(const ps_gpu_plan* P, double* B, double* Np, double* kappa, ps_cfg* cfgs_out)
+// Host side of a finished execution whose results were copied to h (no CUDA calls).
+int plan_unpack(const ps_gpu_plan* P, const double* h, double* B, double* Np, double* kappa, ps_cfg* cfgs_out)
 {
     const int nconf = P->nconf;
-    const double* h = P->hres;
     int err = 0;
     memcpy(&err, h + 10 * (size_t)nconf, sizeof(int));
     for (int q = 0; q < nconf; q++) {
@@ -1793,29 +1917,63 @@ int plan_unpack(const ps_gpu_plan* P, double* B, double* Np, double* kappa, ps_c
 
 int plan_finish(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Np, double* kappa, ps_cfg* cfgs_out)
 {
-    PS_TRY(plan_copy_results(c, P));
+    PS_TRY(plan_copy_results(c, P, P->hres));
     PS_CK(cudaStreamSynchronize(c->stream));
-    if (plan_unpack(P, B, Np, kappa, cfgs_out) != PS_OK)
+    if (plan_unpack(P, P->hres, B, Np, kappa, cfgs_out) != PS_OK)
         return fail(PS_ERR_CUDA, "internal: a derived shell exceeded its launch bound");
     return PS_OK;
 }
 
-// An asynchronous submission: unpacked by a host callback in stream order.
-struct SubmitJob {
-    ps_gpu_ctx* c;
-    const ps_gpu_plan* P;
-    double *B, *Np, *kappa;
-    ps_cfg* cfgs_out;
-};
-
-void CUDART_CB submit_callback(void* arg)
+// Unpacks the asynchronous submissions whose result copies are done, oldest
+// first (with wait, all of them, waiting for each); their page-locked buffers
+// and events go back to the context's spares.
+int drain_pending(ps_gpu_ctx* c, bool wait)
 {
-    SubmitJob* j = (SubmitJob*)arg;
-    if (plan_unpack(j->P, j->B, j->Np, j->kappa, j->cfgs_out) != PS_OK) {
-        int expected = 0;
-        j->c->async_err.compare_exchange_strong(expected, PS_ERR_CUDA);
+    size_t k = 0;
+    int rc = PS_OK;
+    for (; k < c->pending.size(); k++) {
+        PendingSubmit& j = c->pending[k];
+        const cudaError_t e = wait ? cudaEventSynchronize(j.done) : cudaEventQuery(j.done);
+        if (e == cudaErrorNotReady) break;
+        if (e != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "asynchronous submission: %s", cudaGetErrorString(e));
+            break;
+        }
+        if (plan_unpack(j.P, j.host, j.B, j.Np, j.kappa, j.cfgs_out) != PS_OK) {
+            int expected = 0;
+            c->async_err.compare_exchange_strong(expected, PS_ERR_CUDA);
+        }
+        c->spare_host.push_back({j.host, j.host_len});
+        c->spare_events.push_back(j.done);
     }
-    delete j;
+    c->pending.erase(c->pending.begin(), c->pending.begin() + (long)k);
+    return rc;
+}
+
+// Page-locked result buffer of at least len doubles and an event for one submission.
+int submit_slot(ps_gpu_ctx* c, size_t len, double** host, cudaEvent_t* ev)
+{
+    *host = nullptr;
+    for (size_t q = 0; q < c->spare_host.size(); q++)
+        if (c->spare_host[q].second >= len) {
+            *host = c->spare_host[q].first;
+            c->spare_host.erase(c->spare_host.begin() + (long)q);
+            break;
+        }
+    if (!*host) {
+        if (fault_hit(FAULT_ALLOC) || cudaHostAlloc((void**)host, len * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
+            *host = nullptr;
+            return fail(PS_ERR_OOM, "page-locked result buffer of %zu doubles", len);
+        }
+    }
+    if (!c->spare_events.empty()) {
+        *ev = c->spare_events.back();
+        c->spare_events.pop_back();
+    } else if (cudaEventCreateWithFlags(ev, cudaEventDisableTiming) != cudaSuccess) {
+        c->spare_host.push_back({*host, len});
+        return fail(PS_ERR_CUDA, "event creation failed");
+    }
+    return PS_OK;
 }
 
 // Device and pinned memory of a plan (the plan object itself stays).
@@ -1983,7 +2141,7 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
             k_scale_out<T, float><<<148 * 8, 256, 0, c->stream>>>(B.ra, (float*)dst, n3, scale);
         pf.end(fam<T>(KF_GRAD), (double)n3 * (sizeof(T) + (out_is_double ? 8 : 4)), N);
     }
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_status();
     if (e == cudaSuccess && stage) {
         e = cudaMemcpyAsync(out, stage, out_bytes, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -2022,9 +2180,10 @@ int transform_field(ps_gpu_ctx* c, const void* a, const void* b, int is_double, 
 // rounding), on host threads.
 void compose_xhi_dens(ps_gpu_ctx* c, const float* d, const float* x, float* out, size_t n)
 {
-    if (!c->pool) c->pool = new HostPool();
-    const size_t nt = c->pool->n, per = (n + nt - 1) / nt;
-    c->pool->run([=](size_t t) {
+    (void)c;
+    HostPool& pool = HostPool::get();
+    const size_t nt = pool.n, per = (n + nt - 1) / nt;
+    pool.run([=](size_t t) {
         const size_t lo = std::min(n, t * per), hi = std::min(n, lo + per);
         for (size_t i = lo; i < hi; i++) out[i] = (float)((double)d[i] * (1.0 - (double)x[i]));
     });
@@ -2052,7 +2211,7 @@ int load_xhi_dens_host(ps_gpu_ctx* c, const float* dens, const float* xhii, int 
         }
         c->fpin_bytes = 0;
         for (int q = 0; q < 2; q++)
-            if (cudaHostAlloc(&c->fpin[q], bytes, cudaHostAllocDefault) != cudaSuccess) {
+            if (fault_hit(FAULT_ALLOC) || cudaHostAlloc(&c->fpin[q], bytes, cudaHostAllocDefault) != cudaSuccess) {
                 c->fpin[q] = nullptr;
                 return fail(PS_ERR_OOM, "page-locked field buffer of %zu bytes", bytes);
             }
@@ -2110,13 +2269,19 @@ int load_xhi_dens_host(ps_gpu_ctx* c, const float* dens, const float* xhii, int 
     // re-balance: with a composed rows at tc per row and every row's upload at
     // tu per float row (raw rows move two), the load takes about
     // max(tc (nr - split), tu (nr + split)); equal when split/nr = (tc - tu)/(tc + tu)
+    c->load_rows = (long long)nr;
+    c->load_rows_raw = (long long)split;
+    c->load_compose_s = t_comp;
+    c->load_raw_copy_ms = 0.0;
     if (raw_ok) {
         if (split < nr) c->t_comp_row = t_comp / (double)(nr - split);
         if (split > 0) {
             float ms = 0.f;
             if (cudaEventSynchronize(c->ev_raw[1]) == cudaSuccess &&
-                cudaEventElapsedTime(&ms, c->ev_raw[0], c->ev_raw[1]) == cudaSuccess && ms > 0.f)
+                cudaEventElapsedTime(&ms, c->ev_raw[0], c->ev_raw[1]) == cudaSuccess && ms > 0.f) {
                 c->t_up_row = 1e-3 * ms / (2.0 * (double)split);
+                c->load_raw_copy_ms = ms;
+            }
         }
         if (c->t_comp_row > 0.0 && c->t_up_row > 0.0) {
             const double f = (c->t_comp_row - c->t_up_row) / (c->t_comp_row + c->t_up_row);
@@ -2137,6 +2302,8 @@ int load_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int
     const size_t n3 = (size_t)c->N * c->N * c->N;
     const size_t bytes = n3 * (is_double ? 8 : 4);
     int s = -1;
+    c->load_rows = c->load_rows_raw = 0;
+    c->load_compose_s = c->load_raw_copy_ms = 0.0;
     if (mem == PS_MEM_HOST && which == PS_FIELD_XHI_DENS && !is_double && c->methods == PS_FP32_BATCHED)
         return load_xhi_dens_host(c, (const float*)dens, (const float*)xhii, use_only_phase);
     if (mem == PS_MEM_HOST) {
@@ -2211,7 +2378,7 @@ int upload_file(ps_gpu_ctx* c, const char* path, size_t bytes, void* dev)
             rc = fail(PS_ERR_CUDA, "chunk copy: %s", cudaGetErrorString(e));
             break;
         }
-        const size_t got = fread(c->pin[q], 1, len, f);
+        const size_t got = fault_hit(FAULT_READ) ? 0 : fread(c->pin[q], 1, len, f);
         if (got != len) {
             rc = fail(PS_ERR_IO, "%s holds %zu of the %zu bytes of the grid", path, done + got, bytes);
             break;
@@ -2260,9 +2427,15 @@ const char* ps_gpu_strerror(int s)
 
 const char* ps_gpu_last_error(void) { return g_err; }
 
+int ps_gpu_debug_fault(const char* spec) { g_err[0] = 0; return arm_faults(spec); }
+
 int ps_gpu_create(ps_gpu_ctx** out, int nbins, double boxsize, int methods, int device)
 {
     g_err[0] = 0;
+    static std::once_flag env_faults;
+    std::call_once(env_faults, []() {
+        if (const char* e = getenv("PS_FAULT")) arm_faults(e);
+    });
     if (!out) return fail(PS_ERR_ARG, "ctx pointer is NULL");
     *out = nullptr;
     if (!pow2_ok(nbins)) return fail(PS_ERR_UNSUPPORTED, "grid size %d: need a power of two in [16,1024]", nbins);
@@ -2339,10 +2512,25 @@ int ps_gpu_set_field_async(ps_gpu_ctx* c, int which, const void* dens, const voi
     g_err[0] = 0;
     if (!c) return fail(PS_ERR_ARG, "ctx is NULL");
     PS_CK(cudaSetDevice(c->device));
+    PS_TRY(drain_pending(c, false));
     return load_field(c, which, dens, xhii, is_double, mem, use_only_phase);
 }
 
 long long ps_gpu_upload_bytes(const ps_gpu_ctx* c) { return c ? (long long)c->upload_bytes : PS_ERR_ARG; }
+
+int ps_gpu_load_stats(const ps_gpu_ctx* c, ps_load_stats* out)
+{
+    g_err[0] = 0;
+    if (!c || !out) return fail(PS_ERR_ARG, "NULL argument");
+    out->rows = c->load_rows;
+    out->rows_raw = c->load_rows_raw;
+    out->bytes = (long long)c->upload_bytes;
+    out->compose_s = c->load_compose_s;
+    out->raw_copy_ms = c->load_raw_copy_ms;
+    out->next_raw_frac = c->raw_frac;
+    out->host_threads = (int)HostPool::default_threads();
+    return PS_OK;
+}
 
 int ps_gpu_set_field_files(ps_gpu_ctx* c, int which, const char* dens_path, int dens_double, const char* xhii_path,
                            int xhii_double, int use_only_phase)
@@ -2360,7 +2548,8 @@ int ps_gpu_set_field_files(ps_gpu_ctx* c, int which, const char* dens_path, int 
     const size_t n3 = (size_t)c->N * c->N * c->N;
     PS_TRY(ensure_stage(c, n3 * (dp ? 8 : 4)));
     for (int q = 0; q < 2; q++) {
-        if (!c->pin[q] && cudaHostAlloc(&c->pin[q], kFileChunk, cudaHostAllocDefault) != cudaSuccess) {
+        if (!c->pin[q] && (fault_hit(FAULT_ALLOC) ||
+                           cudaHostAlloc(&c->pin[q], kFileChunk, cudaHostAllocDefault) != cudaSuccess)) {
             c->pin[q] = nullptr;
             return fail(PS_ERR_OOM, "page-locked chunk buffer of %zu bytes", kFileChunk);
         }
@@ -2391,7 +2580,7 @@ int ps_gpu_set_field_files(ps_gpu_ctx* c, int which, const char* dens_path, int 
             if (rc == PS_OK) {
                 k_widen<<<148 * 8, 256, 0, c->copy_stream>>>((const float*)c->stage[s ^ 1][r], (double*)c->stage[s][r],
                                                              n3);
-                e = cudaGetLastError();
+                e = launch_status();
                 if (e != cudaSuccess) rc = fail(PS_ERR_CUDA, "widen: %s", cudaGetErrorString(e));
             }
         }
@@ -2431,9 +2620,11 @@ int ps_gpu_polyspectrum_batch(ps_gpu_ctx* c, int method, int nconf, ps_cfg* cfgs
     if (!(c->methods & method)) return fail(PS_ERR_ARG, "method %d not enabled for this context", method);
     PS_CK(cudaSetDevice(c->device));
     PS_TRY(timed_begin(c));
+    const std::vector<ps_cfg> in(cfgs, cfgs + nconf);
     int rc = method == PS_FP64_PLAIN ? plain_batch(c, nconf, cfgs, B, Npoly, kappa)
                                      : batched(c, nconf, cfgs, B, Npoly, kappa);
     if (rc != PS_OK) return rc;
+    remember_npoly(c, method, nconf, in.data(), Npoly);
     return timed_end(c);
 }
 
@@ -2488,13 +2679,20 @@ int ps_gpu_grad(ps_gpu_ctx* c, int method, int n, const double* k, const double*
         g.kmin[l] = kmin[l];
         g.kmax[l] = kmax[l];
     }
-    // B and the polygon count of the configuration (sum I = N^3 * Npoly)
-    double Bv = 0.0, Np = 0.0;
-    {
+    // the polygon count of the configuration (sum I = N^3 * Npoly): from an
+    // earlier evaluation on this context (counts do not depend on the field),
+    // else evaluated here
+    double Np = 0.0;
+    const auto known = c->npoly_cache.find(npoly_key(method, g));
+    if (known != c->npoly_cache.end()) {
+        Np = known->second;
+    } else {
         ps_cfg g2 = g;
+        double Bv = 0.0;
         int rc = method == PS_FP64_PLAIN ? plain_batch(c, 1, &g2, &Bv, &Np, nullptr)
                                          : batched(c, 1, &g2, &Bv, &Np, nullptr);
         if (rc != PS_OK) return rc;
+        remember_npoly(c, method, 1, &g, &Np);
     }
     PS_TRY(timed_begin(c));
     std::vector<std::vector<Shell>> legs;
@@ -2658,6 +2856,7 @@ void ps_gpu_plan_destroy(ps_gpu_plan* P)
     if (P->ctx) {
         cudaSetDevice(P->ctx->device);
         cudaStreamSynchronize(P->ctx->stream);  // submissions still reading it
+        drain_pending(P->ctx, true);            // and those not yet unpacked
         P->ctx->plans.erase(P);
     }
     plan_free(P);
@@ -2678,14 +2877,20 @@ int ps_gpu_plan_submit(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly, 
     PS_CK(cudaSetDevice(c->device));
     if ((P->flags & PS_PLAN_GRAPH) && c->prof_on) PS_TRY(plan_enqueue(c, P));
     else PS_TRY(plan_run(c, P));
-    PS_TRY(plan_copy_results(c, P));
-    SubmitJob* j = new SubmitJob{c, P, B, Npoly, kappa, cfgs_out};
-    const cudaError_t e = cudaLaunchHostFunc(c->stream, submit_callback, j);
-    if (e != cudaSuccess) {
-        delete j;
-        return fail(PS_ERR_CUDA, "cudaLaunchHostFunc: %s", cudaGetErrorString(e));
+    const size_t len = 10 * (size_t)P->nconf + 1;
+    double* h = nullptr;
+    cudaEvent_t ev = nullptr;
+    PS_TRY(submit_slot(c, len, &h, &ev));
+    int rc = plan_copy_results(c, P, h);
+    if (rc == PS_OK && cudaEventRecord(ev, c->stream) != cudaSuccess) rc = fail(PS_ERR_CUDA, "event record failed");
+    if (rc != PS_OK) {
+        cudaStreamSynchronize(c->stream);  // no copy still writes h
+        c->spare_host.push_back({h, len});
+        c->spare_events.push_back(ev);
+        return rc;
     }
-    return PS_OK;
+    c->pending.push_back(PendingSubmit{P, h, len, ev, B, Npoly, kappa, cfgs_out});
+    return drain_pending(c, false);
 }
 
 int ps_gpu_plan_launch(ps_gpu_ctx* c, ps_gpu_plan* P)
@@ -2716,6 +2921,20 @@ int ps_gpu_plan_results(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly,
     return plan_finish(c, P, B, Npoly, kappa, cfgs_out);
 }
 
+int ps_gpu_plan_results_device(ps_gpu_ctx* c, ps_gpu_plan* P, double* dst)
+{
+    g_err[0] = 0;
+    if (!c || !P || !dst) return fail(PS_ERR_ARG, "NULL argument");
+    if (P->ctx != c) return fail(PS_ERR_ARG, "plan belongs to another context");
+    if (P->method != PS_FP32_BATCHED) return fail(PS_ERR_UNSUPPORTED, "results of a PS_FP32_BATCHED plan only");
+    if (P->nconf == 0) return PS_OK;
+    PS_CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)P->nconf;
+    PS_CK(cudaMemcpyAsync(dst, P->dres, 16 * n, cudaMemcpyDeviceToDevice, c->stream));
+    PS_CK(cudaMemcpyAsync(dst + 2 * n, P->dwb, 48 * n, cudaMemcpyDeviceToDevice, c->stream));
+    return PS_OK;
+}
+
 int ps_gpu_synchronize(ps_gpu_ctx* c)
 {
     g_err[0] = 0;
@@ -2723,6 +2942,7 @@ int ps_gpu_synchronize(ps_gpu_ctx* c)
     PS_CK(cudaSetDevice(c->device));
     PS_CK(cudaStreamSynchronize(c->copy_stream));
     PS_CK(cudaStreamSynchronize(c->stream));
+    PS_TRY(drain_pending(c, true));
     const int e = c->async_err.exchange(0);
     if (e != PS_OK) return fail(e, "internal: a derived shell exceeded its launch bound (asynchronous execution)");
     return PS_OK;
@@ -2836,6 +3056,13 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    drain_pending(c, true);
+    for (auto& j : c->pending) {  // copies that failed: their buffers only
+        cudaFreeHost(j.host);
+        cudaEventDestroy(j.done);
+    }
+    for (auto& hb : c->spare_host) cudaFreeHost(hb.first);
+    for (cudaEvent_t e : c->spare_events) cudaEventDestroy(e);
     for (ps_gpu_plan* P : c->plans) {  // plans outliving their context keep only their host part
         plan_release(P);
         P->ctx = nullptr;
@@ -2859,7 +3086,6 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
         if (c->ev_fpin[q]) cudaEventDestroy(c->ev_fpin[q]);
         if (c->ev_raw[q]) cudaEventDestroy(c->ev_raw[q]);
     }
-    delete c->pool;
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);

@@ -96,39 +96,21 @@ def _all_gather(dist, arr: np.ndarray) -> list[np.ndarray]:
     return [o.cpu().numpy() for o in out]
 
 
-def evaluate_sharded(ctx, cfgs, method: int | None = None, evaluate=None) -> ShardedResult:
-    """Evaluate `cfgs` over all ranks of the default process group (or alone
-    when none is initialised).  `evaluate(sub_cfgs) -> (B, Npoly, cfgs_out)`
-    defaults to ctx.batch with `method` (PS_FP32_BATCHED)."""
-    from . import PS_FP32_BATCHED, ps_cfg
-    dist = _dist()
-    rank, world = (dist.get_rank(), dist.get_world_size()) if dist else (0, 1)
-    n = len(cfgs)
-    parts = partition(cfgs, world)
+def _gather(dist, parts, rank, n, local, err):
+    """Status exchange, then one all-gather of every rank's results, unpacked
+    into the caller's order.  `local` = (B, Npoly, cfgs_out) of this rank's
+    share or None; `err` = this rank's exception or None."""
     mine = parts[rank]
-    if evaluate is None:
-        m = PS_FP32_BATCHED if method is None else method
-
-        def evaluate(sub):
-            B, Np, _, out = ctx.batch(sub, m)
-            return B, Np, out
     payload = np.zeros((max(len(p) for p in parts) if parts else 0, PAYLOAD))
-    status = 0
-    try:
-        if mine:
-            sub = (ps_cfg * len(mine))()
-            for j, i in enumerate(mine):
-                C.memmove(C.byref(sub[j]), C.byref(cfgs[i]), C.sizeof(ps_cfg))
-            B, Np, out = evaluate(sub)
-            for j, i in enumerate(mine):
-                payload[j, 0] = i
-                payload[j, 1] = B[j]
-                payload[j, 2] = Np[j]
-                payload[j, 3:11] = list(out[j].kmin)
-                payload[j, 11:19] = list(out[j].kmax)
-    except Exception as e:  # joins the status exchange below, then raises everywhere
-        status = 1
-        err = e
+    status = 1 if err is not None else 0
+    if err is None and mine:
+        B, Np, out = local
+        for j, i in enumerate(mine):
+            payload[j, 0] = i
+            payload[j, 1] = B[j]
+            payload[j, 2] = Np[j]
+            payload[j, 3:11] = list(out[j].kmin)
+            payload[j, 11:19] = list(out[j].kmax)
     if dist:
         flags = _all_gather(dist, np.array([float(status)]))
         failed = [q for q, f in enumerate(flags) if f[0] != 0.0]
@@ -149,3 +131,106 @@ def evaluate_sharded(ctx, cfgs, method: int | None = None, evaluate=None) -> Sha
             B[i], Np[i] = blk[j, 1], blk[j, 2]
             kmin[i], kmax[i] = blk[j, 3:11], blk[j, 11:19]
     return ShardedResult(B, Np, kmin, kmax, parts)
+
+
+def share(cfgs, mine):
+    """The configurations of indices `mine` as a ps_cfg array."""
+    from . import ps_cfg
+    sub = (ps_cfg * max(len(mine), 1))()
+    for j, i in enumerate(mine):
+        C.memmove(C.byref(sub[j]), C.byref(cfgs[i]), C.sizeof(ps_cfg))
+    return sub if mine else sub[:0]
+
+
+def evaluate_sharded(ctx, cfgs, method: int | None = None, evaluate=None) -> ShardedResult:
+    """Evaluate `cfgs` over all ranks of the default process group (or alone
+    when none is initialised).  `evaluate(sub_cfgs) -> (B, Npoly, cfgs_out)`
+    defaults to ctx.batch with `method` (PS_FP32_BATCHED)."""
+    from . import PS_FP32_BATCHED
+    dist = _dist()
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist else (0, 1)
+    parts = partition(cfgs, world)
+    mine = parts[rank]
+    if evaluate is None:
+        m = PS_FP32_BATCHED if method is None else method
+
+        def evaluate(sub):
+            B, Np, _, out = ctx.batch(sub, m)
+            return B, Np, out
+    local, err = None, None
+    try:
+        if mine:
+            local = evaluate(share(cfgs, mine))
+    except Exception as e:  # joins the status exchange, then raises everywhere
+        err = e
+    return _gather(dist, parts, rank, len(cfgs), local, err)
+
+
+class ShardedPlan:
+    """A configuration list split over the ranks of the default process group
+    (whole theta sweeps, balanced as `partition` does), each rank holding one
+    plan of its share (PS_FP32_BATCHED, CUDA graph, optionally autotuned).
+    execute() runs this rank's plan on the field loaded last and returns every
+    rank's results through one all-gather; launch() / gather() split that into
+    the stream work and the exchange.  `make_plan(sub_cfgs)` replaces
+    ctx.plan (tests)."""
+
+    def __init__(self, ctx, cfgs, autotune: bool = True, graph: bool = True, make_plan=None):
+        dist = _dist()
+        self.dist = dist
+        self.rank, self.world = (dist.get_rank(), dist.get_world_size()) if dist else (0, 1)
+        self.n = len(cfgs)
+        self.parts = partition(cfgs, self.world)
+        self._err = None
+        mine = self.parts[self.rank]
+        self.plan = None
+        err = None
+        try:
+            if mine:
+                sub = share(cfgs, mine)
+                self.plan = make_plan(sub) if make_plan else ctx.plan(sub, graph=graph, autotune=autotune)
+        except Exception as e:
+            err = e
+        # every rank learns whether every plan was made
+        mine_flag = np.array([float(err is not None)])
+        flags = _all_gather(dist, mine_flag) if dist else [mine_flag]
+        failed = [q for q, f in enumerate(flags) if f[0] != 0.0]
+        if failed:
+            if err is not None:
+                raise ShardError(f"rank {self.rank} failed to plan its share: {err}") from err
+            raise ShardError(f"ranks {failed} failed to plan their share")
+
+    @property
+    def band(self) -> int:
+        """Largest |component| of a mode this rank's share reads (-1: no share)."""
+        return self.plan.band if self.plan is not None else -1
+
+    def launch(self):
+        """Queue this rank's plan execution (results stay on the device).  A
+        failure is kept and reported by the next gather(), on every rank."""
+        try:
+            if self.plan is not None:
+                self.plan.launch()
+        except Exception as e:
+            self._err = e
+
+    def gather(self) -> ShardedResult:
+        """Results of the latest launch on every rank (waits; one all-gather)."""
+        local, err = None, self._err
+        self._err = None
+        try:
+            if err is None and self.plan is not None:
+                B, Np, _, out = self.plan.results()
+                local = (B, Np, out)
+        except Exception as e:
+            err = e
+        return _gather(self.dist, self.parts, self.rank, self.n, local, err)
+
+    def execute(self) -> ShardedResult:
+        self.launch()
+        return self.gather()
+
+    def close(self):
+        if self.plan is not None:
+            self.plan.close()
+            self.plan = None

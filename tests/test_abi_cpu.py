@@ -108,3 +108,15 @@ def test_make_configs_matches_oracle_run(ps, ora, case):
         np.testing.assert_array_equal(hi, r.kmax)
     if n == 3 and p["equilateral"] != 1 and p["num_values"] > 1:
         np.testing.assert_array_equal(th, r.theta)
+
+
+def test_fault_spec_parsing(ps):
+    """ps_gpu_debug_fault arms the host-side injector without touching a GPU;
+    malformed specs are refused."""
+    lib = ps.lib()
+    for good in (b"alloc:1", b"read:3", b"launch:2", b"alloc:5,read:1", b""):
+        assert lib.ps_gpu_debug_fault(good) == 0, good
+    for bad in (b"alloc", b"alloc:0", b"alloc:-2", b"disk:1", b"alloc:x", b"alloc:1,", b"launch:1x"):
+        assert lib.ps_gpu_debug_fault(bad) == -1, bad
+        assert b"fault spec" in lib.ps_gpu_last_error()
+    assert lib.ps_gpu_debug_fault(None) == 0

@@ -126,3 +126,74 @@ def test_failing_rank_raises_everywhere(ps, tmp_path):
         msg = open(os.path.join(str(tmp_path), f"r{r}.err")).read()
         assert "fail" in msg
     assert "planted failure" in open(os.path.join(str(tmp_path), "r1.err")).read()
+
+
+class FakePlan:
+    """Stand-in for a ps.Plan of a share: launch() computes, results() returns."""
+
+    def __init__(self, sub, fail=False):
+        self.sub = sub
+        self.fail = fail
+        self.res = None
+
+    def launch(self):
+        if self.fail:
+            raise RuntimeError("planted launch failure")
+        self.res = fake_evaluate(self.sub)
+
+    def results(self):
+        B, Np, out = self.res
+        return B, Np, None, out
+
+    def close(self):
+        pass
+
+
+def _plan_worker(rank, world, port, outdir, fail_rank):
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import datetime
+
+    import torch.distributed as dist
+
+    import polyspectrum_b200 as ps
+    from polyspectrum_b200.multi import ShardError, ShardedPlan
+    from test_multi_cpu import FakePlan, bench_like_cfgs
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        cfgs = bench_like_cfgs(ps)
+        sp = ShardedPlan(None, cfgs, make_plan=lambda sub: FakePlan(sub, fail=rank == fail_rank))
+        try:
+            for _ in range(2):  # two steps, the same collective sequence on every rank
+                res = sp.execute()
+            np.savez(os.path.join(outdir, f"r{rank}.npz"), B=res.B, npoly=res.npoly, kmin=res.kmin, kmax=res.kmax)
+        except ShardError as e:
+            with open(os.path.join(outdir, f"r{rank}.err"), "w") as f:
+                f.write(str(e))
+        sp.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,fail_rank", [(2, -1), (3, -1), (2, 0)])
+def test_sharded_plan_steps(ps, tmp_path, world, fail_rank):
+    """ShardedPlan: each rank plans its share once, every step gathers all
+    results in the caller's order; a rank whose launch fails makes every rank
+    raise at the same step."""
+    import torch.multiprocessing as mp
+
+    from polyspectrum_b200.multi import evaluate_sharded
+    cfgs = bench_like_cfgs(ps)
+    serial = evaluate_sharded(None, cfgs, evaluate=fake_evaluate)
+    mp.spawn(_plan_worker, args=(world, _free_port(), str(tmp_path), fail_rank), nprocs=world, join=True)
+    for r in range(world):
+        if fail_rank >= 0:
+            msg = open(os.path.join(str(tmp_path), f"r{r}.err")).read()
+            assert "fail" in msg
+            continue
+        got = np.load(os.path.join(str(tmp_path), f"r{r}.npz"))
+        np.testing.assert_array_equal(got["B"], serial.B)
+        np.testing.assert_array_equal(got["npoly"], serial.npoly)
+        np.testing.assert_array_equal(got["kmin"], serial.kmin)
