@@ -30,7 +30,8 @@ DRIVER = os.path.join(PKG, "ps_run")
 KBENCH = os.path.join(PKG, "ps_kbench")
 CREATE_INI_SRC = os.path.join(PKG, "driver", "ps_create_ini.c")
 CREATE_INI = os.path.join(PKG, "ps_create_ini")
-SOURCES = ["ps_api.cu", "ps_inst_f32.cu", "ps_inst_f64.cu", "ps_noalloc.cu"]
+SOURCES = ["ps_api.cu", "ps_inst_f32.cu", "ps_inst_f64.cu", "ps_inst_f32_mixed.cu", "ps_inst_f64_mixed.cu",
+           "ps_noalloc.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off"]

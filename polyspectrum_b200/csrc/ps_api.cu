@@ -130,6 +130,11 @@ cudaError_t launch_status()
     case 384: { constexpr int NN = 384; BODY; } break; \
     case 512: { constexpr int NN = 512; BODY; } break; \
     case 1024: { constexpr int NN = 1024; BODY; } break; \
+    case 48: { constexpr int NN = 48; BODY; } break;   \
+    case 60: { constexpr int NN = 60; BODY; } break;   \
+    case 96: { constexpr int NN = 96; BODY; } break;   \
+    case 300: { constexpr int NN = 300; BODY; } break; \
+    case 600: { constexpr int NN = 600; BODY; } break; \
     default: return fail(PS_ERR_UNSUPPORTED, "grid size %d not supported", N); \
     }
 
@@ -341,7 +346,14 @@ struct ps_gpu_ctx {
 namespace {
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
-bool pow2_ok(int n) { return n >= 16 && n <= 1024 && (n & (n - 1)) == 0; }
+// Grid sizes a context runs on: powers of two 16..1024 and 48, 60, 96, 192,
+// 300, 320, 384, 600 (2^a 3^b 5^c; the reference's FFTW takes any N).
+bool grid_size_ok(int n)
+{
+    for (int q : {16, 32, 48, 60, 64, 96, 128, 192, 256, 300, 320, 384, 512, 600, 1024})
+        if (q == n) return true;
+    return false;
+}
 double ref_pi() { return acos(-1.0); }  // filter.c:19
 
 // Pencil-tile width (complex elements per row segment) of the pencil kernels.
@@ -357,6 +369,11 @@ template <typename T> int pw(int N)
     case 320: return PencilGeom<T, 320>::W;
     case 384: return PencilGeom<T, 384>::W;
     case 512: return PencilGeom<T, 512>::W;
+    case 48: return PencilGeom<T, 48>::W;
+    case 60: return PencilGeom<T, 60>::W;
+    case 96: return PencilGeom<T, 96>::W;
+    case 300: return PencilGeom<T, 300>::W;
+    case 600: return PencilGeom<T, 600>::W;
     default: return PencilGeom<T, 1024>::W;
     }
 }
@@ -2438,7 +2455,9 @@ int ps_gpu_create(ps_gpu_ctx** out, int nbins, double boxsize, int methods, int 
     });
     if (!out) return fail(PS_ERR_ARG, "ctx pointer is NULL");
     *out = nullptr;
-    if (!pow2_ok(nbins)) return fail(PS_ERR_UNSUPPORTED, "grid size %d: need a power of two in [16,1024]", nbins);
+    if (!grid_size_ok(nbins))
+        return fail(PS_ERR_UNSUPPORTED, "grid size %d: supported are the powers of two 16..1024 and 48, 60, 96, "
+                                        "192, 300, 320, 384, 600", nbins);
     if (!(boxsize > 0.0) || !std::isfinite(boxsize)) return fail(PS_ERR_ARG, "box size must be positive");
     if (!(methods & (PS_FP64_PLAIN | PS_FP32_BATCHED)) || (methods & ~(PS_FP64_PLAIN | PS_FP32_BATCHED)))
         return fail(PS_ERR_ARG, "methods mask %d invalid", methods);

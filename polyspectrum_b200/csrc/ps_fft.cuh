@@ -2,7 +2,8 @@
 //
 // A transform of length N is done by TPF = N/R threads.  Thread t holds
 // a[e] = x[t + TPF*e] ("canonical layout") on entry and X[t + TPF*e] on exit.
-// N is a power of two, or 3 or 5 times one (sub-grid transforms).  Passes are
+// N is a power of two, or 3 or 5 times one, for the register passes below;
+// other lengths 2^a 3^b 5^c take the shared-memory passes (GenericPlan).  Passes are
 // radix-R (for N = f 2^k, R = f 2^r: radix-2^r passes, one of a smaller power
 // of two if needed, then one radix-R pass last); each thread does R/Rp
 // butterflies per pass.  Pass p with radix Rp and span Ns (product of the
@@ -204,11 +205,23 @@ template <int N, int R> struct RadixPlan {
     static_assert(F == 1 || R2 >= 2 || N == R, "mixed lengths need a power-of-two part in R");
 };
 
-// Elements per thread used for each transform length (3 2^k and 5 2^k: the
-// odd factor times 4, 16 or 32 threads per transform).
+// Elements per thread used for each register-plan length (3 2^k and 5 2^k:
+// the odd factor times 2 or 4, 4 to 32 threads per transform).
 template <int N> struct DefaultRadix {
-    static constexpr int value = N == 96 ? 12 : N == 160 ? 20 : N == 192 ? 12 : N == 320 ? 20 : N == 384 ? 12
+    static constexpr int value = N == 24 ? 6 : N == 40 ? 10 : N == 48 ? 12 : N == 80 ? 20 : N == 96 ? 12
+                               : N == 160 ? 20 : N == 192 ? 12 : N == 320 ? 20 : N == 384 ? 12
                                : N <= 16 ? N : (N == 32 || N == 64 || N == 128 || N == 512) ? 8 : 16;
+};
+
+// Thread layout of a transform of length L: R elements per thread, TPF
+// threads per transform (a power of two, so rows pack whole warps).  Lengths
+// whose odd part is 1, 3 or 5 use the register plan (TPF = L / R); the others
+// ("ragged": 30, 60, 150, 300, 600, ...) take TPF threads with R = ceil(L/TPF)
+// slots each, the last ones past L idle, and the shared-memory passes.
+template <int L> struct LenKind {
+    __host__ __device__ static constexpr int odd_of(int n) { return n % 2 ? n : odd_of(n / 2); }
+    static constexpr bool RAGGED = !(odd_of(L) == 1 || odd_of(L) == 3 || odd_of(L) == 5);
+    static constexpr int RAGGED_TPF = L <= 32 ? 4 : L <= 64 ? 8 : L <= 160 ? 16 : 32;
 };
 
 // Synchronisation between passes: the whole CTA (pencil kernels, whose
@@ -278,11 +291,128 @@ __device__ __forceinline__ void fft_passes(V (&a)[R], int t, Acc& sm, const V* _
     }
 }
 
-// Host side: the Stockham table of RadixPlan<N, R> (forward sign), from
-// exp(-2 pi i m / M) evaluated in long double.
-template <typename V, int N, int R> inline void stockham_table(V* out)
+// Pass sequence of lengths N = 2^a 3^b 5^c whose odd part does not fit one
+// register pass ("ragged" transforms, e.g. 60, 150, 300, 600): radix-8 passes,
+// one radix-4 or -2 pass for the rest of the power of two, then one radix-3
+// pass per factor 3 and one radix-5 pass per factor 5.  Such transforms keep
+// their data in shared memory between passes; each thread does the
+// butterflies v = t, t + TPF, ... of a pass.
+template <int N> struct GenericPlan {
+    __host__ __device__ static constexpr int pow2_of(int n) { return n % 2 ? 1 : 2 * pow2_of(n / 2); }
+    __host__ __device__ static constexpr int count_of(int n, int f) { return n % f ? 0 : 1 + count_of(n / f, f); }
+    __host__ __device__ static constexpr int ilog2(int v) { return v > 1 ? 1 + ilog2(v / 2) : 0; }
+    static constexpr int A = ilog2(pow2_of(N));
+    static constexpr int B3 = count_of(N, 3), C5 = count_of(N, 5);
+    static constexpr int P8 = A / 3, PR = A % 3 ? 1 : 0;
+    static constexpr int P = P8 + PR + B3 + C5;
+    __host__ __device__ static constexpr int radix(int p)
+    {
+        return p < P8 ? 8 : (p < P8 + PR ? (A % 3 == 2 ? 4 : 2) : (p < P8 + PR + B3 ? 3 : 5));
+    }
+    __host__ __device__ static constexpr int span(int p)
+    {
+        int s = 1;
+        for (int q = 0; q < p; q++) s *= radix(q);
+        return s;
+    }
+    __host__ __device__ static constexpr int tw_off(int p)
+    {
+        int o = 0;
+        for (int q = 0; q < p; q++) o += span(q) * (radix(q) - 1);
+        return o;
+    }
+    __host__ __device__ static constexpr int product()
+    {
+        int s = 1;
+        for (int q = 0; q < P; q++) s *= radix(q);
+        return s;
+    }
+    static_assert(product() == N, "length must be 2^a 3^b 5^c");
+};
+
+// Whether a transform of N elements over TPF threads with R elements each
+// runs the register passes (RadixPlan; N = R * TPF with the odd part of N in
+// R) or the shared-memory passes of GenericPlan.
+template <int N, int R, int TPF> struct UseRegisterPlan {
+    __host__ __device__ static constexpr int odd_of(int n) { return n % 2 ? n : odd_of(n / 2); }
+    static constexpr bool value = R * TPF == N && odd_of(R) == odd_of(N) &&
+                                  (odd_of(R) == 1 || odd_of(R) == 3 || odd_of(R) == 5) &&
+                                  (odd_of(R) == 1 || R / odd_of(R) >= 2 || N == R);
+};
+
+// The passes of GenericPlan<N> on the transform held in shared memory behind
+// `sm` (positions 0..N-1); each thread does butterflies t, t + TPF, ...
+template <typename V, int N, int R, int TPF, bool INV, int P_ = 0, class Acc, class Sync>
+__device__ __forceinline__ void generic_passes(Acc& sm, int t, const V* __restrict__ twt, const Sync& sync)
 {
-    using Plan = RadixPlan<N, R>;
+    using Plan = GenericPlan<N>;
+    if constexpr (P_ < Plan::P) {
+        constexpr int Rp = Plan::radix(P_);
+        constexpr int Ns = Plan::span(P_);
+        constexpr int NB = N / Rp;                   // butterflies of the pass
+        constexpr int BPT = (NB + TPF - 1) / TPF;    // per thread (the last ones partly idle)
+        V b[BPT][Rp];
+#pragma unroll
+        for (int u = 0; u < BPT; u++) {
+            const int v = t + TPF * u;
+            if (v < NB) {
+#pragma unroll
+                for (int q = 0; q < Rp; q++) b[u][q] = sm.ld(v + q * NB);
+            }
+        }
+        sync();
+#pragma unroll
+        for (int u = 0; u < BPT; u++) {
+            const int v = t + TPF * u;
+            if (v < NB) {
+                const int k = v % Ns;
+                if constexpr (Ns > 1) {
+                    const V* tp = twt + Plan::tw_off(P_) + k * (Rp - 1);
+#pragma unroll
+                    for (int q = 1; q < Rp; q++) {
+                        V w = tp[q - 1];
+                        if constexpr (INV) w.y = -w.y;
+                        b[u][q] = cmul(b[u][q], w);
+                    }
+                }
+                Dft<Rp, INV>::run(b[u]);
+                const int j = (v / Ns) * Ns * Rp + k;
+#pragma unroll
+                for (int q = 0; q < Rp; q++) sm.st(j + q * Ns, b[u][q]);
+            }
+        }
+        sync();
+        generic_passes<V, N, R, TPF, INV, P_ + 1>(sm, t, twt, sync);
+    }
+}
+
+// A transform of length N held by TPF threads, R elements each (canonical
+// layout a[e] = x[t + TPF e]; with R * TPF > N the entries past N are not
+// part of the transform and are left as they are).  Register passes when the
+// length allows them, else shared-memory passes; either way the buffer behind
+// `sm` holds N elements.
+template <typename V, int N, int R, int TPF, bool INV, class Acc, class Sync>
+__device__ __forceinline__ void fft_any(V (&a)[R], int t, Acc& sm, const V* __restrict__ twt, const Sync& sync)
+{
+    if constexpr (UseRegisterPlan<N, R, TPF>::value) {
+        fft_passes<V, N, R, INV>(a, t, sm, twt, sync);
+    } else {
+#pragma unroll
+        for (int e = 0; e < R; e++)
+            if (t + TPF * e < N) sm.st(t + TPF * e, a[e]);
+        sync();
+        generic_passes<V, N, R, TPF, INV>(sm, t, twt, sync);
+#pragma unroll
+        for (int e = 0; e < R; e++)
+            if (t + TPF * e < N) a[e] = sm.ld(t + TPF * e);
+        sync();
+    }
+}
+
+// Host side: the Stockham table of a pass plan (forward sign), from
+// exp(-2 pi i m / M) evaluated in long double.
+template <typename V, class Plan> inline void plan_table(V* out)
+{
     const long double two_pi = 6.283185307179586476925286766559005768L;
     for (int p = 0; p < Plan::P; p++) {
         const int Rp = Plan::radix(p), Ns = Plan::span(p);
@@ -295,6 +425,13 @@ template <typename V, int N, int R> inline void stockham_table(V* out)
             }
     }
 }
+template <typename V, int N, int R> inline void stockham_table(V* out) { plan_table<V, RadixPlan<N, R>>(out); }
+// the table of the transform fft_any<V, N, R, TPF> runs
+template <typename V, int N, int R, int TPF> inline void transform_table(V* out)
+{
+    if constexpr (UseRegisterPlan<N, R, TPF>::value) plan_table<V, RadixPlan<N, R>>(out);
+    else plan_table<V, GenericPlan<N>>(out);
+}
 
 // Shared-memory accessor for pencil passes: W transforms interleaved, element
 // `pos` of transform `lane` at s[pos*W + lane] (conflict-free when W*sizeof(V)
@@ -304,6 +441,8 @@ template <typename V, int W> struct SmemInterleaved {
     int lane;
     template <int Rp, int Ns> __device__ __forceinline__ void st(int pos, V v) { s[pos * W + lane] = v; }
     template <int Rp, int Ns> __device__ __forceinline__ V ld(int pos) const { return s[pos * W + lane]; }
+    __device__ __forceinline__ void st(int pos, V v) { s[pos * W + lane] = v; }
+    __device__ __forceinline__ V ld(int pos) const { return s[pos * W + lane]; }
 };
 
 // Shared-memory accessor for row passes: one row per transform, XOR-swizzled

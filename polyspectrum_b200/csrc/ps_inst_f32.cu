@@ -2,5 +2,5 @@
 #include "ps_launch.cuh"
 
 namespace ps {
-PS_INSTANTIATE_L3(float)
+PS_INSTANTIATE_L3_POW2(float)
 }  // namespace ps

@@ -2,5 +2,5 @@
 #include "ps_launch.cuh"
 
 namespace ps {
-PS_INSTANTIATE_L3(double)
+PS_INSTANTIATE_L3_POW2(double)
 }  // namespace ps

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <vector>
 #include <cmath>
+#include <algorithm>
 #include "ps_launch.cuh"
 
 namespace ps {
@@ -23,6 +24,7 @@ int launch_fail(cudaError_t e, const char* what)
     fprintf(stderr, "%s: %s\n", what, cudaGetErrorString(e));
     return 1;
 }
+template struct L3<float, 320>;
 template struct L3<float, 384>;
 template struct L3<float, 512>;
 }
@@ -65,6 +67,55 @@ template <int M> Tables<float> make_tables()
     return Tables<float>{a, b, c};
 }
 static int rup(int a, int b) { return (a + b - 1) / b * b; }
+
+// Row Stockham table of the pair kernel variant <M, RX>.
+template <int M, int RX> float2* pair_row_table()
+{
+    using G = RowGeom<float, M, RX>;
+    std::vector<float2> hr(M / 2);
+    transform_table<float2, M / 2, G::R, G::TPF>(hr.data());
+    float2* d;
+    CK(cudaMalloc(&d, M / 2 * 8));
+    CK(cudaMemcpy(d, hr.data(), M / 2 * 8, cudaMemcpyHostToDevice));
+    return d;
+}
+
+// Mean time of `reps` launches of the pair kernel variant <M, RX, KEEP> on
+// legs of bands ba, bb (arrays wa, wb of strides Sa, Sb) into w3 (stride S).
+template <int M, int RX, bool KEEP>
+double time_pair(int reps, const float2* wa, int Sa, int ba, const float2* wb, int Sb, int bb, float2* w3, int S,
+                 int bc, const float2* twpp)
+{
+    using G = RowGeom<float, M, RX>;
+    using PGm = PairGeom<float, M, RX, KEEP>;
+    const float2* twr = pair_row_table<M, RX>();
+    const size_t smem = PGm::smem(2, ba + 1, bb + 1);
+    auto kern = k_pair_z<float, M, RX, KEEP>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::THREADS, smem));
+    const int nrows = M * M, tiles = (nrows + G::WZ - 1) / G::WZ;
+    const int grid = std::min(tiles, std::max(per_sm, 1) * sms);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int it = 0; it < 3; it++)
+        kern<<<grid, G::THREADS, smem>>>(wa, Sa, ba + 1, wb, Sb, bb + 1, w3, S, bc + 1, nrows, twr, twpp);
+    CK(cudaEventRecord(e0));
+    for (int it = 0; it < reps; it++)
+        kern<<<grid, G::THREADS, smem>>>(wa, Sa, ba + 1, wb, Sb, bb + 1, w3, S, bc + 1, nrows, twr, twpp);
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    printf("pair_z@%d R=%d keep=%d: %.4f ms  (%d threads, %d CTAs/SM, %zu B smem)\n", M, G::R, (int)KEEP,
+           ms / reps, G::THREADS, per_sm, smem);
+    CK(cudaFree((void*)twr));
+    return ms / reps;
+}
 struct Timer {
     std::vector<cudaEvent_t> ev; std::vector<double> acc; int k = 0;
     Timer(int n) : ev(n + 1), acc(n, 0.0) { for (auto& e : ev) CK(cudaEventCreate(&e)); }
@@ -129,5 +180,19 @@ int main(int argc, char** argv)
     }
     CK(cudaDeviceSynchronize());
     for (int q = 0; q < NK; q++) printf("%-18s %.4f ms\n", names[q], tm.acc[q] / reps);
+
+    // pair kernel variants: the 384-point group above, and a 320-point group
+    // (leg bands 52 and 77, closing band 128: the shapes of the third sweep)
+    time_pair<384, 0, false>(reps, wa, Sa, ba, wb, Sb, bb, w3, S, bc, T3.twpp);
+    time_pair<384, 0, true>(reps, wa, Sa, ba, wb, Sb, bb, w3, S, bc, T3.twpp);
+    time_pair<384, 24, true>(reps, wa, Sa, ba, wb, Sb, bb, w3, S, bc, T3.twpp);
+    {
+        const int a2 = 52, b2 = 77, c2 = 128;
+        const int Sa2 = rup(a2 + 1, 16), Sb2 = rup(b2 + 1, 16), S2 = rup(c2 + 1, 16);
+        Tables<float> T2 = make_tables<320>();
+        time_pair<320, 0, false>(reps, wa, Sa2, a2, wb, Sb2, b2, w3, S2, c2, T2.twpp);
+        time_pair<320, 0, true>(reps, wa, Sa2, a2, wb, Sb2, b2, w3, S2, c2, T2.twpp);
+        time_pair<320, 20, true>(reps, wa, Sa2, a2, wb, Sb2, b2, w3, S2, c2, T2.twpp);
+    }
     return 0;
 }

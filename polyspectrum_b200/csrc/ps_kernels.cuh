@@ -33,14 +33,20 @@ constexpr int MAX_DOT_SHELLS = 16;
 // Pencils per CTA in the strided passes: one 128-byte segment of a row.
 template <typename T> struct PencilWidth { static constexpr int value = 128 / (int)sizeof(V2<T>); };
 
-// Elements per thread of the pencil (strided-axis) transforms: radix 16 for
-// FP32 at N = 512 so a CTA of 16 pencils is 512 threads.
-template <typename T, int N> struct PencilRadix {
-    static constexpr int value = (sizeof(T) == 4 && N == 512) ? 16 : DefaultRadix<N>::value;
+// Threads per pencil (strided-axis) transform: N / (register-plan radix),
+// with radix 16 for FP32 at N = 512 so a CTA of 16 pencils is 512 threads;
+// ragged lengths take LenKind's thread count (64 for FP64 pencils above 512).
+template <typename T, int N> struct PencilThreads {
+    static constexpr int value = LenKind<N>::RAGGED ? ((sizeof(T) == 8 && N > 512) ? 64 : LenKind<N>::RAGGED_TPF)
+                               : N / ((sizeof(T) == 4 && N == 512) ? 16 : DefaultRadix<N>::value);
 };
 template <typename T, int N> struct PencilGeom {
-    static constexpr int R = PencilRadix<T, N>::value;
-    static constexpr int TPF = N / R;
+    static constexpr int TPF = PencilThreads<T, N>::value;
+    static constexpr int R = (N + TPF - 1) / TPF;
+    // element e of thread t is position t + TPF e of the transform; with
+    // R * TPF > N (ragged lengths) the positions past N are idle slots
+    static constexpr bool FULL = R * TPF == N;
+    __device__ static constexpr bool live(int pos) { return FULL || pos < N; }
     // one 128-byte segment per row, whole warps per CTA, at most 512 threads
     // (so an epilogue keeps 16 FP64 accumulators in registers)
     static constexpr int W0 = PencilWidth<T>::value * TPF >= 32 ? PencilWidth<T>::value : 32 / TPF;
@@ -65,26 +71,37 @@ template <typename T, int NH> struct RowRadix {
     static constexpr int value = NH == 160 ? 10 : !POW2 ? DefaultRadix<NH>::value
                                : NH <= 16 ? NH : ((sizeof(T) == 4 && NH == 512) ? 16 : 8);
 };
-template <typename T, int N> struct RowGeom {
+// RX > 0 overrides the elements per thread of a register-plan row length
+// (the pair kernel's variants).
+template <typename T, int N, int RX = 0> struct RowGeom {
     static constexpr int NH = N / 2;
-    static constexpr int R = RowRadix<T, NH>::value;
-    static constexpr int TPF = NH / R;
+    static constexpr int TPF = LenKind<NH>::RAGGED ? LenKind<NH>::RAGGED_TPF : NH / (RX > 0 ? RX : RowRadix<T, NH>::value);
+    static constexpr int R = (NH + TPF - 1) / TPF;
+    // element e of thread t is pair t + TPF e of the row; with R * TPF > NH
+    // (ragged lengths) the pairs past NH are idle slots
+    static constexpr bool FULL = R * TPF == NH;
+    __device__ static constexpr bool live(int n) { return FULL || n < NH; }
     static constexpr int EPC = 16 / (int)sizeof(V2<T>);  // complex elements per 16-byte copy
     // rows per CTA (tile): up to 256 threads and 32 rows, and as many as fit
     // in 227 KB of shared memory with two double-buffered full-length inputs
     static constexpr int WZ0 = (256 / TPF) < 32 ? (256 / TPF) : 32;
     static constexpr size_t ROW_BYTES =
-        (size_t)(NH + 4 * ((NH + 1 + EPC - 1) / EPC * EPC)) * sizeof(V2<T>);
+        (size_t)((NH < 16 ? NH : (NH + 15) / 16 * 16) + 4 * ((NH + 1 + EPC - 1) / EPC * EPC)) * sizeof(V2<T>);
     static constexpr int WZ_FIT = (int)((227 * 1024 - (size_t)(2 * NH + 2) * sizeof(V2<T>)) / ROW_BYTES);
     __host__ __device__ static constexpr int pow2_floor(int v) { return v >= 2 ? 2 * pow2_floor(v / 2) : 1; }
-    static constexpr int WZ = pow2_floor(WZ0 < WZ_FIT ? WZ0 : WZ_FIT);
+    // and a divisor of the N^2 rows, so whole tiles cover the grid
+    __host__ __device__ static constexpr int pow2_dividing(int v, int cap) { return cap > 1 && v % cap ? pow2_dividing(v, cap / 2) : cap; }
+    static constexpr int WZ = pow2_dividing(N * N, pow2_floor(WZ0 < WZ_FIT ? WZ0 : WZ_FIT));
     static constexpr int THREADS = TPF * WZ;
     // shared memory: row Stockham table [NH], pre/post twiddles W_N^k, k <= NH
     // [NH+2], per-row exchange buffers [WZ][NH], then the input stages
     static constexpr size_t TWR_OFF = 0;
     static constexpr size_t TWPP_OFF = TWR_OFF + (size_t)NH * sizeof(V2<T>);
     static constexpr size_t ROWBUF_OFF = TWPP_OFF + (size_t)(NH + 2) * sizeof(V2<T>);
-    static constexpr size_t STAGE_OFF = ROWBUF_OFF + (size_t)WZ * NH * sizeof(V2<T>);
+    // row exchange buffers hold whole swizzle blocks of SmemRow (16 elements:
+    // its XOR stays inside a block, which a ragged NH may end in the middle of)
+    static constexpr int ROWBUF = NH < 16 ? NH : (NH + 15) / 16 * 16;
+    static constexpr size_t STAGE_OFF = ROWBUF_OFF + (size_t)WZ * ROWBUF * sizeof(V2<T>);
     // input stage pitch (elements) for rows of hv valid entries
     __host__ __device__ static constexpr int pitch(int hv) { return (hv + EPC - 1) / EPC * EPC; }
     // dynamic shared memory of a kernel with `ninputs` double-buffered inputs
@@ -208,10 +225,13 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     unsigned bits = 0u;
     if (pencil_live) {
         if (mode == LOAD_PLAIN) {
-            bits = (1u << G::R) - 1u;
+#pragma unroll
+            for (int e = 0; e < G::R; e++)
+                if (G::live(t + G::TPF * e)) bits |= 1u << e;
         } else {
 #pragma unroll 1
             for (int e = 0; e < G::R; e++) {
+                if (!G::live(t + G::TPF * e)) continue;
                 const int mx = lattice_freq(t + G::TPF * e, N);
                 if (abs(mx) <= sh.band && shell_bit(sh, mx, my, mz)) bits |= 1u << e;
             }
@@ -228,11 +248,11 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
         }
         a[e] = v;
     }
-    fft_passes<V, N, G::R, true>(a, t, sm, tw, BlockSync{});
+    fft_any<V, N, G::R, G::TPF, true>(a, t, sm, tw, BlockSync{});
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int i = t + G::TPF * e;
-        if (!quad || i <= N / 2) dst[((size_t)i * nj + j) * dst_stride + h] = a[e];
+        if (G::live(i) && (!quad || i <= N / 2)) dst[((size_t)i * nj + j) * dst_stride + h] = a[e];
     }
 }
 
@@ -260,28 +280,30 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
     for (int e = 0; e < G::R; e++) {
         const int j = t + G::TPF * e;
         const int jr = quad && j > N / 2 ? N - j : j;
-        a[e] = (jband >= N / 2 || abs(lattice_freq(j, N)) <= jband) ? base[(size_t)jr * stride] : czero<V>();
+        a[e] = G::live(j) && (jband >= N / 2 || abs(lattice_freq(j, N)) <= jband) ? base[(size_t)jr * stride]
+                                                                                  : czero<V>();
     }
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
     __syncthreads();
     SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), w};
-    fft_passes<V, N, G::R, INV>(a, t, sm, tw, BlockSync{});
+    fft_any<V, N, G::R, G::TPF, INV>(a, t, sm, tw, BlockSync{});
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int j = t + G::TPF * e;
         // jout < N/2: rows with |my| > jout are read by no later pass and not stored
-        if ((!quad || j <= N / 2) && (jout >= N / 2 || abs(lattice_freq(j, N)) <= jout)) base[(size_t)j * stride] = a[e];
+        if (G::live(j) && (!quad || j <= N / 2) && (jout >= N / 2 || abs(lattice_freq(j, N)) <= jout))
+            base[(size_t)j * stride] = a[e];
     }
 }
 
 // ------------------------------------------------------------------ row helpers
 // A CTA works on tiles of WZ consecutive (i,j) rows; row w of a tile is done
 // by threads [w*TPF, (w+1)*TPF), which synchronise among themselves only.
-template <typename T, int N> struct RowCtx {
-    using G = RowGeom<T, N>;
+template <typename T, int N, int RX = 0> struct RowCtx {
+    using G = RowGeom<T, N, RX>;
     using V = V2<T>;
     int w, t;
-    V* rowbuf;       // this row's exchange buffer [NH]
+    V* rowbuf;       // this row's exchange buffer [ROWBUF >= NH]
     const V* twr;    // Stockham table of the NH-point transform
     const V* twpp;   // W_N^k, k <= NH (r2c / c2r pre- and post-processing)
     RowSync<G::TPF> sync;
@@ -293,7 +315,7 @@ template <typename T, int N> struct RowCtx {
         twpp = stage_table<V>(smem + G::TWPP_OFF, twpp_g, G::NH + 1);
         w = threadIdx.x / G::TPF;
         t = threadIdx.x % G::TPF;
-        rowbuf = reinterpret_cast<V*>(smem + G::ROWBUF_OFF) + w * G::NH;
+        rowbuf = reinterpret_cast<V*>(smem + G::ROWBUF_OFF) + w * G::ROWBUF;
         sync.bar = 1 + w;
         if constexpr (G::TPF >= 32) {
             sync.mask = 0xffffffffu;
@@ -306,16 +328,20 @@ template <typename T, int N> struct RowCtx {
 
 // c2r of one spectrum row held in shared memory (entries h < hv, zero above)
 // into registers, canonical layout: a[e] = (x[2n], x[2n+1]), n = t + TPF*e.
-template <typename T, int N>
-__device__ __forceinline__ void c2r_row(const V2<T>* zr, int hv, RowCtx<T, N>& rc,
-                                        V2<T> (&a)[RowGeom<T, N>::R])
+template <typename T, int N, int RX = 0>
+__device__ __forceinline__ void c2r_row(const V2<T>* zr, int hv, RowCtx<T, N, RX>& rc,
+                                        V2<T> (&a)[RowGeom<T, N, RX>::R])
 {
-    using G = RowGeom<T, N>;
+    using G = RowGeom<T, N, RX>;
     using V = V2<T>;
     constexpr int NH = G::NH;
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int k = rc.t + G::TPF * e;
+        if (!G::live(k)) {
+            a[e] = czero<V>();
+            continue;
+        }
         const V zk = k < hv ? zr[k] : czero<V>();
         const V zm = (NH - k) < hv ? cconj(zr[NH - k]) : czero<V>();
         const V A = cadd(zk, zm);
@@ -323,23 +349,24 @@ __device__ __forceinline__ void c2r_row(const V2<T>* zr, int hv, RowCtx<T, N>& r
         a[e] = V{A.x - B.y, A.y + B.x};
     }
     SmemRow<V> sm{rc.rowbuf};
-    fft_passes<V, NH, G::R, true>(a, rc.t, sm, rc.twr, rc.sync);
+    fft_any<V, NH, G::R, G::TPF, true>(a, rc.t, sm, rc.twr, rc.sync);
     rc.sync();
 }
 
 // r2c of a real row held in registers (canonical pairs), writing h < hout.
-template <typename T, int N>
-__device__ __forceinline__ void r2c_row(V2<T> (&a)[RowGeom<T, N>::R], RowCtx<T, N>& rc, V2<T>* __restrict__ xo,
+template <typename T, int N, int RX = 0>
+__device__ __forceinline__ void r2c_row(V2<T> (&a)[RowGeom<T, N, RX>::R], RowCtx<T, N, RX>& rc, V2<T>* __restrict__ xo,
                                         int hout)
 {
-    using G = RowGeom<T, N>;
+    using G = RowGeom<T, N, RX>;
     using V = V2<T>;
     constexpr int NH = G::NH;
     SmemRow<V> sm{rc.rowbuf};
-    fft_passes<V, NH, G::R, false>(a, rc.t, sm, rc.twr, rc.sync);
+    fft_any<V, NH, G::R, G::TPF, false>(a, rc.t, sm, rc.twr, rc.sync);
     rc.sync();
 #pragma unroll
-    for (int e = 0; e < G::R; e++) sm.st(rc.t + G::TPF * e, a[e]);
+    for (int e = 0; e < G::R; e++)
+        if (G::live(rc.t + G::TPF * e)) sm.st(rc.t + G::TPF * e, a[e]);
     rc.sync();
     const T half = (T)0.5;
     for (int k = rc.t; k <= NH && k < hout; k += G::TPF) {
@@ -405,6 +432,7 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
         const T* arow = aux ? aux + row * N : nullptr;
 #pragma unroll
         for (int e = 0; e < G::R; e++) {
+            if (!G::live(rc.t + G::TPF * e)) continue;
             const int n2 = 2 * (rc.t + G::TPF * e);
             T x0 = ipow(a[e].x, power), x1 = ipow(a[e].y, power);
             if (epi == EPI_STORE) {
@@ -529,25 +557,29 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS,
         const unsigned char* ra = sa + (size_t)w0 * N * eb;
         const unsigned char* rb = gb ? sb + (size_t)w0 * N * eb : nullptr;
 #pragma unroll
-        for (int e = 0; e < G::R; e++) a[e] = load_pair<T>(kind, ra, rb, t0 + G::TPF * e);
+        for (int e = 0; e < G::R; e++)
+            a[e] = G::live(t0 + G::TPF * e) ? load_pair<T>(kind, ra, rb, t0 + G::TPF * e) : czero<V>();
         r2c_row<T, N>(a, rc, dst + row * dst_stride, hout);
     } else {
         if (kind == SRC_T) {
             const V* xr = reinterpret_cast<const V*>((const T*)a_src + row * N);
 #pragma unroll
-            for (int e = 0; e < G::R; e++) a[e] = xr[t0 + G::TPF * e];
+            for (int e = 0; e < G::R; e++) a[e] = G::live(t0 + G::TPF * e) ? xr[t0 + G::TPF * e] : czero<V>();
         } else if (vec) {
             // both values of a pair in one 8- or 16-byte load per array
             const int eb = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 4 : 8;
             const unsigned char* ra = reinterpret_cast<const unsigned char*>(a_src) + row * N * eb;
             const unsigned char* rb = b_src ? reinterpret_cast<const unsigned char*>(b_src) + row * N * eb : nullptr;
 #pragma unroll
-            for (int e = 0; e < G::R; e++) a[e] = load_pair<T>(kind, ra, rb, t0 + G::TPF * e);
+            for (int e = 0; e < G::R; e++)
+                a[e] = G::live(t0 + G::TPF * e) ? load_pair<T>(kind, ra, rb, t0 + G::TPF * e) : czero<V>();
         } else {
 #pragma unroll
             for (int e = 0; e < G::R; e++) {
                 const size_t n2 = row * N + 2 * (t0 + G::TPF * e);
-                a[e] = V{load_real<T>(kind, a_src, b_src, n2), load_real<T>(kind, a_src, b_src, n2 + 1)};
+                a[e] = G::live(t0 + G::TPF * e)
+                           ? V{load_real<T>(kind, a_src, b_src, n2), load_real<T>(kind, a_src, b_src, n2 + 1)}
+                           : czero<V>();
             }
         }
         RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
@@ -561,20 +593,34 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS,
 // transformed forward again: c2r(A) * c2r(B) -> r2c, all along l, so the real
 // product D_a*D_b (or D_a^2 when B is NULL) never leaves the SM.  Output rows
 // keep h < hout.  Persistent and double-buffered like k_inv_z.
-template <typename T, int N>
-__global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
+//   RX   : elements per thread of the row transforms (0: RowRadix's choice)
+//   KEEP : c2r(A)'s values wait in shared memory (each thread its own slots,
+//          no synchronisation) while c2r(B) runs, so one row transform is
+//          live in registers at a time instead of two
+template <typename T, int N, int RX, bool KEEP> struct PairGeom {
+    using G = RowGeom<T, N, RX>;
+    // dynamic shared memory: the row kernels' layout, then the keep buffers
+    __host__ __device__ static constexpr size_t smem(int ninputs, int hva, int hvb)
+    {
+        return G::smem(ninputs, hva, hvb) + (KEEP ? (size_t)G::WZ * G::ROWBUF * sizeof(V2<T>) : 0);
+    }
+};
+
+template <typename T, int N, int RX = 0, bool KEEP = false>
+__global__ void __launch_bounds__(RowGeom<T, N, RX>::THREADS)
     k_pair_z(const V2<T>* __restrict__ srcA, int sa, int hva, const V2<T>* __restrict__ srcB, int sb,
              int hvb, V2<T>* __restrict__ dst, int ds, int hout, int nrows, const V2<T>* __restrict__ twr_g,
              const V2<T>* __restrict__ twpp_g)
 {
-    using G = RowGeom<T, N>;
+    using G = RowGeom<T, N, RX>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
+    RowCtx<T, N, RX> rc(smem_raw, twr_g, twpp_g);
     const bool two = srcB != nullptr;
     const int PA = G::pitch(hva), PB = two ? G::pitch(hvb) : 0;
     V* stA = reinterpret_cast<V*>(smem_raw + G::STAGE_OFF);
     V* stB = stA + 2 * G::WZ * PA;
+    V* keep = stB + 2 * G::WZ * PB + rc.w * G::ROWBUF;  // KEEP: this row's slots
     const int ntiles = (nrows + G::WZ - 1) / G::WZ;
     int tile = blockIdx.x;
     if (tile < ntiles) {
@@ -600,18 +646,30 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS)
             continue;
         }
         V a[G::R];
-        c2r_row<T, N>(stA + st * G::WZ * PA + rc.w * PA, hva, rc, a);
+        c2r_row<T, N, RX>(stA + st * G::WZ * PA + rc.w * PA, hva, rc, a);
         if (two) {
-            V b[G::R];
-            c2r_row<T, N>(stB + st * G::WZ * PB + rc.w * PB, hvb, rc, b);
+            if constexpr (KEEP) {
 #pragma unroll
-            for (int e = 0; e < G::R; e++) a[e] = V{a[e].x * b[e].x, a[e].y * b[e].y};
+                for (int e = 0; e < G::R; e++)
+                    if (G::live(rc.t + G::TPF * e)) keep[rc.t + G::TPF * e] = a[e];
+                c2r_row<T, N, RX>(stB + st * G::WZ * PB + rc.w * PB, hvb, rc, a);
+#pragma unroll
+                for (int e = 0; e < G::R; e++) {
+                    const V q = G::live(rc.t + G::TPF * e) ? keep[rc.t + G::TPF * e] : czero<V>();
+                    a[e] = V{a[e].x * q.x, a[e].y * q.y};
+                }
+            } else {
+                V b[G::R];
+                c2r_row<T, N, RX>(stB + st * G::WZ * PB + rc.w * PB, hvb, rc, b);
+#pragma unroll
+                for (int e = 0; e < G::R; e++) a[e] = V{a[e].x * b[e].x, a[e].y * b[e].y};
+            }
         } else {
 #pragma unroll
             for (int e = 0; e < G::R; e++) a[e] = V{a[e].x * a[e].x, a[e].y * a[e].y};
         }
         // the products sit in canonical layout as (x[2n], x[2n+1]): r2c input as is
-        r2c_row<T, N>(a, rc, dst + row * ds, hout);
+        r2c_row<T, N, RX>(a, rc, dst + row * ds, hout);
         __syncthreads();
     }
 }
@@ -691,7 +749,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
 #pragma unroll
     for (int e = 0; e < G::R; e++) {
         const int i = t + G::TPF * e;
-        a[e] = data[((size_t)(quad && i > N / 2 ? N - i : i) * nj + j) * stride + h];
+        a[e] = G::live(i) ? data[((size_t)(quad && i > N / 2 ? N - i : i) * nj + j) * stride + h] : czero<V>();
     }
     // sums: the shell bits depend on indices only and are found before the
     // transform (16 bits per mode, two modes per register)
@@ -703,7 +761,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
         for (int e = 0; e < G::R; e++) {
             const int mx = lattice_freq(t + G::TPF * e, N);
             unsigned b = 0u;
-            if (col_ok) {
+            if (col_ok && G::live(t + G::TPF * e)) {
                 if (lut) {
                     const int r2 = mx * mx + my * my + mz * mz;
                     b = r2 < lut_size ? (unsigned)__ldg(lut + r2) : 0u;
@@ -717,7 +775,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
     const V* tw = stage_table<V>(smem_raw, tw_g, N);
     __syncthreads();
     SmemInterleaved<V, G::W> sm{reinterpret_cast<V*>(smem_raw + G::TW_BYTES), w};
-    fft_passes<V, N, G::R, false>(a, t, sm, tw, BlockSync{});
+    fft_any<V, N, G::R, G::TPF, false>(a, t, sm, tw, BlockSync{});
     if constexpr (!DOT) {
         unsigned keep = (1u << G::R) - 1u;
         if (epi == SPEC_MASK_ADD) {
@@ -726,6 +784,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
             if (col_ok) {
 #pragma unroll 1
                 for (int e = 0; e < G::R; e++) {
+                    if (!G::live(t + G::TPF * e)) continue;
                     const int mx = lattice_freq(t + G::TPF * e, N);
                     if (in_band(sh, mx, my, mz) && shell_bit(sh, mx, my, mz)) keep |= 1u << e;
                 }
@@ -735,6 +794,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
 #pragma unroll
         for (int e = 0; e < G::R; e++) {
             const int i = t + G::TPF * e;
+            if (!G::live(i)) continue;
             if (jband < N / 2 && abs(lattice_freq(i, N)) > jband) continue;
             V v = a[e];
             if (epi == SPEC_STORE_PHASE) {

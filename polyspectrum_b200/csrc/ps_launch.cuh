@@ -1,6 +1,6 @@
 // Launch wrappers of the pass kernels for one (precision, N), instantiated
-// explicitly in ps_inst_f32.cu / ps_inst_f64.cu so the heavy unrolled kernels
-// compile in parallel translation units.
+// explicitly in ps_inst_f32.cu / ps_inst_f64.cu (and the *_mixed.cu units) so
+// the heavy unrolled kernels compile in parallel translation units.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -68,8 +68,8 @@ template <typename T, int N> struct L3 {
     // host copies of the tables for this N
     static void host_tables(V* twp, V* twr)
     {
-        stockham_table<V, N, PG::R>(twp);
-        stockham_table<V, N / 2, RG::R>(twr);
+        transform_table<V, N, PG::R, PG::TPF>(twp);
+        transform_table<V, N / 2, RG::R, RG::TPF>(twr);
     }
     // quad: the xy-quadrant layout of data even in x and y ([i <= N/2][j <= N/2][h])
     // nsrc: grid size of the source spectrum src (0: N; a larger field grid
@@ -183,9 +183,11 @@ template <typename T, int N> struct L3 {
     }
 };
 
-// Grid sizes: the powers of two a context runs on, and 3 2^k / 5 2^k sizes
-// for the alias-free sub-grids of pair groups.
-#define PS_INSTANTIATE_L3(T)          \
+// Grid sizes.  Powers of two 16..1024, the 3 2^k / 5 2^k sizes of the
+// alias-free sub-grids of pair groups (192, 320, 384), and further grid sizes
+// 2^a 3^b 5^c a context may run on (48, 96: register plans; 60, 300, 600:
+// shared-memory passes) - instantiated in two translation units per precision.
+#define PS_INSTANTIATE_L3_POW2(T)     \
     template struct L3<T, 16>;        \
     template struct L3<T, 32>;        \
     template struct L3<T, 64>;        \
@@ -197,16 +199,28 @@ template <typename T, int N> struct L3 {
     template struct L3<T, 512>;       \
     template struct L3<T, 1024>;
 
+#define PS_INSTANTIATE_L3_MIXED(T)    \
+    template struct L3<T, 48>;        \
+    template struct L3<T, 60>;        \
+    template struct L3<T, 96>;        \
+    template struct L3<T, 300>;       \
+    template struct L3<T, 600>;
+
 #define PS_EXTERN_L3(T)                  \
     extern template struct L3<T, 16>;    \
     extern template struct L3<T, 32>;    \
+    extern template struct L3<T, 48>;    \
+    extern template struct L3<T, 60>;    \
     extern template struct L3<T, 64>;    \
+    extern template struct L3<T, 96>;    \
     extern template struct L3<T, 128>;   \
     extern template struct L3<T, 192>;   \
     extern template struct L3<T, 256>;   \
+    extern template struct L3<T, 300>;   \
     extern template struct L3<T, 320>;   \
     extern template struct L3<T, 384>;   \
     extern template struct L3<T, 512>;   \
+    extern template struct L3<T, 600>;   \
     extern template struct L3<T, 1024>;
 
 }  // namespace ps

@@ -446,9 +446,16 @@ int main(int argc, char **argv)
         fprintf(stderr, "Not supported option. Please use 'DENS', 'XHII' or 'XHI_DENS'\n");
         exit(EXIT_FAILURE);
     }
-    if (c.grid_size < 16 || c.grid_size > 1024 || (c.grid_size & (c.grid_size - 1))) {
-        fprintf(stderr, "ps_run: gridsize %d: need a power of two in [16, 1024]\n", c.grid_size);
-        exit(EXIT_FAILURE);
+    {
+        /* the grid sizes the library's transforms take (ps_gpu_create refuses others) */
+        static const int sizes[] = {16, 32, 48, 60, 64, 96, 128, 192, 256, 300, 320, 384, 512, 600, 1024};
+        int ok = 0;
+        for (size_t q = 0; q < sizeof(sizes) / sizeof(sizes[0]); q++) ok |= sizes[q] == c.grid_size;
+        if (!ok) {
+            fprintf(stderr, "ps_run: gridsize %d: supported are the powers of two 16..1024 and 48, 60, 96, 192, "
+                            "300, 320, 384, 600\n", c.grid_size);
+            exit(EXIT_FAILURE);
+        }
     }
     printf("Option: %s\t", c.which_field);
     const size_t n3 = (size_t)c.grid_size * c.grid_size * c.grid_size;

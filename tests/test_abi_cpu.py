@@ -55,8 +55,9 @@ def test_strerror_and_bad_arguments(ps):
     assert lib.ps_gpu_strerror(0) == b"ok"
     assert lib.ps_gpu_strerror(-8) == b"undefined in the reference"
     h = C.c_void_p()
-    assert lib.ps_gpu_create(C.byref(h), 100, 100.0, 1, -1) == -7  # not a power of two
-    assert b"power of two" in lib.ps_gpu_last_error()
+    assert lib.ps_gpu_create(C.byref(h), 100, 100.0, 1, -1) == -7  # not a supported size
+    assert b"supported are" in lib.ps_gpu_last_error()
+    assert lib.ps_gpu_create(C.byref(h), 72, 100.0, 1, -1) == -7
     assert lib.ps_gpu_create(C.byref(h), 64, -1.0, 1, -1) == -1
     assert lib.ps_gpu_create(C.byref(h), 64, 100.0, 0, -1) == -1
     assert lib.ps_gpu_create(None, 64, 100.0, 1, -1) == -1

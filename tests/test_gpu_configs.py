@@ -128,3 +128,40 @@ def test_config_1024_power_and_triangles(gpu_lib):
     assert ok, rel.max()
     np.testing.assert_array_equal(got_N, np.rint(N64))
     assert np.all(N32[: n // 2] > 0)  # every shell below Nyquist holds modes
+
+
+@pytest.mark.parametrize("n", [300, 600])
+def test_config_mixed_radix_grid(gpu_lib, ora, n):
+    """300^3 and 600^3 grids (2^a 3 5^2 cells, the sizes of the reference's
+    accuracy study linked from its README): an XHI_DENS field in a box of
+    n Mpc/h (ionised spheres at the benchmark's number density, lognormal
+    density), phase-only, DERIVED binning, a 16-bin theta sweep with
+    k1 = 0.3, k2 = 0.6 h/Mpc.  Batched FP32 against plain FP64 on every bin
+    (1e-5 relative, no absolute floor; counts exact; DERIVED ranges
+    identical); at 300^3 two bins also against the oracle."""
+    ps = gpu_lib
+    box = float(n)
+    dens, xhii = synth.xhi_dens_inputs(n, box, int(round(32000 * (box / 400.0) ** 3)), 3, 2.0, 4)
+    cfgs, k, th = ps.read_params_to_kvectors(n, box, 3, k1=0.3, k2=0.6, num_values=16,
+                                             kbinningCase=ps.PS_BIN_DERIVED)
+    with ps.Context(n, box) as ctx:
+        ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+        B64, N64, _, o64 = ctx.batch(cfgs, ps.PS_FP64_PLAIN)
+        B32, N32, kap, o32 = ctx.batch(cfgs, ps.PS_FP32_BATCHED, kappa=True)
+    np.testing.assert_array_equal(N32, np.rint(N64))
+    assert np.all(N32 > 0)
+    rel = np.abs(B32 - B64) / np.abs(B64)
+    assert rel.max() <= 1e-5, (rel, kap)
+    for q in range(16):
+        for l in range(3):
+            assert o32[q].kmin[l] == o64[q].kmin[l] and o32[q].kmax[l] == o64[q].kmax[l]
+    if n == 300:
+        p = ora.RunParams(grid_size=n, box_size=box, which_field=2, use_only_phase=1, n=3, equilateral=0,
+                          k1=0.3, k2=0.6, num_values=16, kbinwidth=1.0, kbinning=1)
+        for t in (3, 11):
+            ref = ora.ora_run(p, dens, xhii, max_cfg=1, first=t)
+            assert abs(B64[t] - ref.B[0]) <= 1e-9 * abs(ref.B[0]), (t, B64[t], ref.B[0])
+            assert abs(B32[t] - ref.B[0]) <= 1e-5 * abs(ref.B[0]), (t, B32[t], ref.B[0])
+            assert N32[t] == np.rint(ref.npoly[0])
+            np.testing.assert_array_equal([o32[t].kmin[l] for l in range(3)], ref.kmin[0])
+            np.testing.assert_array_equal([o32[t].kmax[l] for l in range(3)], ref.kmax[0])

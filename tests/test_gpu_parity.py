@@ -517,3 +517,28 @@ def test_host_xhi_dens_composition(gpu_lib, methods):
     for g in [got, got_async] + got_pinned:
         np.testing.assert_array_equal(g[0], want[0])
         np.testing.assert_array_equal(g[1], want[1])
+
+
+@pytest.mark.parametrize("n_grid", [48, 60, 96])
+@pytest.mark.parametrize("method", [1, 2], ids=["plain64", "batched32"])
+@pytest.mark.parametrize("kb", [0, 1, 2, 3])
+def test_mixed_radix_grid_sizes(gpu_lib, ora, n_grid, method, kb):
+    """Grids of 2^a 3^b 5^c cells other than powers of two (the reference's
+    FFTW transforms any N, fft.c:30-36,50-56): 48 and 96 run the register
+    passes with a radix-3 factor, 60 the shared-memory passes (odd part 15).
+    A theta sweep of the XHI_DENS field in every binning case (phase-only with
+    DERIVED binning), and the power spectrum over all shells."""
+    box = 150.0
+    kf = 2 * np.pi / box
+    case = dict(n=3, equilateral=0, k1=3.3 * kf, k2=5.1 * kf, num_values=6, theta=0.0,
+                kbinwidth=1.0, kbinning=kb, dcos_theta=0.2, use_only_phase=1 if kb == 1 else 0, which_field=2)
+    ref, got = run_both(gpu_lib, ora, n_grid, box, case, method)
+    check(ref, got, method, f"N={n_grid} kb={kb}")
+    np.testing.assert_array_equal(got.kmin, ref.kmin)
+    np.testing.assert_array_equal(got.kmax, ref.kmax)
+    if kb == 0:
+        p2 = dict(n=2, equilateral=0, k1=0.0, k2=0.0, num_values=2, theta=0.0, kbinwidth=1.0, kbinning=0,
+                  dcos_theta=0.2, use_only_phase=0, which_field=0)
+        ref, got = run_both(gpu_lib, ora, n_grid, box, p2, method)
+        assert len(got.B) == n_grid // 2
+        check(ref, got, method, f"N={n_grid} power spectrum")
