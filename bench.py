@@ -14,7 +14,13 @@ A step runs the forward transform of the field and all 64 configurations.
 
 Prints one JSON line (rank 0).  `value` is device-timed with inputs resident
 in HBM; `e2e` is the same step through the C-ABI from pinned host inputs with
-the host->device copies and the result read-back inside the timed region.
+the host->device copies and the result read-back inside the timed region;
+`parity` checks the timed results against plain FP64 (all 64) and the
+reference (configuration 0).  With --gpus N > 1 (one process per GPU under
+torchrun) the step is the sharded path with weak scaling: 64 configurations
+per rank (the four sweeps once per rank, shifted by -0.005 r h/Mpc for copy
+r), each rank's share one plan, one NCCL all-gather of the results per step;
+--replicas runs N independent copies of the 64-configuration step instead.
 """
 from __future__ import annotations
 
