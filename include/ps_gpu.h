@@ -160,6 +160,14 @@ int ps_gpu_polyspectrum_batch(ps_gpu_ctx *ctx, int method, int nconf, ps_cfg *cf
  * rounding.  Choices are kept per context and can be exported / imported
  * (ps_gpu_tune_export / ps_gpu_tune_import) so later runs use the same sizes. */
 #define PS_PLAN_AUTOTUNE 4
+/* Polygon counts of a pair group whose shells are all r^2 intervals (DEFAULT,
+ * GIVEN and DERIVED binning) are counted exactly in integers by default:
+ * every leg pair (m_a, m_b), S_a reduced to orbit representatives under the
+ * 48 axis permutations and sign flips, histogrammed by |m_a + m_b|^2 (wrapped
+ * on the grid as the reference's cyclic sums wrap).  PS_PLAN_FFT_COUNTS
+ * counts with FP64 transforms of the unit shells instead (the reference's
+ * dataflow; WATKINSON shells always do).  Both give the same integers. */
+#define PS_PLAN_FFT_COUNTS 8
 typedef struct ps_gpu_plan ps_gpu_plan;
 int ps_gpu_plan_create(ps_gpu_ctx *ctx, int method, int nconf, const ps_cfg *cfgs, int flags,
                        ps_gpu_plan **plan);

@@ -307,9 +307,9 @@ class Context:
         return B, Np, kap, arr
 
     def plan(self, cfgs, method: int = PS_FP32_BATCHED, graph: bool = True, kappa: bool = False,
-             autotune: bool = False):
+             autotune: bool = False, fft_counts: bool = False):
         """A reusable plan of these configurations (ps_gpu_plan_create)."""
-        return Plan(self, cfgs, method, graph, kappa, autotune)
+        return Plan(self, cfgs, method, graph, kappa, autotune, fft_counts)
 
     def set_spectrum_band(self, band: int):
         """Later loads compute only modes with |components| <= band (-1: all)."""
@@ -364,20 +364,22 @@ class Context:
 PS_PLAN_GRAPH = 1
 PS_PLAN_KAPPA = 2
 PS_PLAN_AUTOTUNE = 4
+PS_PLAN_FFT_COUNTS = 8
 
 
 class Plan:
     """ps_gpu_plan: a batch planned once, executed per field (CUDA graph replay
     with graph=True)."""
 
-    def __init__(self, ctx: Context, cfgs, method=PS_FP32_BATCHED, graph=True, kappa=False, autotune=False):
+    def __init__(self, ctx: Context, cfgs, method=PS_FP32_BATCHED, graph=True, kappa=False, autotune=False,
+                 fft_counts=False):
         arr = cfgs if isinstance(cfgs, C.Array) else (ps_cfg * len(cfgs))(*cfgs)
         self.ctx = ctx
         self.n = len(arr)
         self.kappa = kappa
         h = C.c_void_p()
         flags = ((PS_PLAN_GRAPH if graph else 0) | (PS_PLAN_KAPPA if kappa else 0)
-                 | (PS_PLAN_AUTOTUNE if autotune else 0))
+                 | (PS_PLAN_AUTOTUNE if autotune else 0) | (PS_PLAN_FFT_COUNTS if fft_counts else 0))
         _check(lib().ps_gpu_plan_create(ctx.handle, method, self.n, arr, flags, C.byref(h)))
         self._h = h
 

@@ -15,7 +15,8 @@ against the unmodified reference itself in its cpu-baseline leg.  Tolerance:
 |dB| <= 1e-5 |B| with no absolute floor, polygon counts exact, DERIVED
 k-ranges bit-identical.  The same 64 configurations loaded from device arrays
 (the composition then runs in the r2c loader instead of on host threads) give
-bit-identical results."""
+bit-identical results, and counting polygons with FP64 transforms of the unit
+shells instead of the exact enumeration gives the same counts and B."""
 import numpy as np
 import pytest
 
@@ -51,8 +52,14 @@ def test_headline_sweep_matches_oracle(gpu_lib, ora):
         ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, torch.from_numpy(dens).cuda(), torch.from_numpy(xhii).cuda(),
                          use_only_phase=1)
         Bd, Npd, _, _ = ctx.batch(arr, ps.PS_FP32_BATCHED)
+        # the counts of the FP64 unit-shell transforms (the reference's dataflow)
+        plan = ctx.plan(arr, graph=False, fft_counts=True)
+        Bf, Npf, _, _ = plan.execute()
+        plan.close()
     np.testing.assert_array_equal(Bd, B)
     np.testing.assert_array_equal(Npd, Np)
+    np.testing.assert_array_equal(Npf, Np)
+    np.testing.assert_array_equal(Bf, B)
     assert np.all(np.isfinite(B)) and np.all(Np > 0)
     assert np.all(np.isfinite(kap)) and np.all(kap >= 1.0)
     for pi, ti in CHECKED:

@@ -542,3 +542,42 @@ def test_mixed_radix_grid_sizes(gpu_lib, ora, n_grid, method, kb):
         ref, got = run_both(gpu_lib, ora, n_grid, box, p2, method)
         assert len(got.B) == n_grid // 2
         check(ref, got, method, f"N={n_grid} power spectrum")
+
+
+def _plan_both_counts(ps, ctx, cfgs):
+    """(B, Npoly) of a plan counting by enumeration and of one counting by
+    FP64 unit-shell transforms."""
+    out = []
+    for fft in (False, True):
+        plan = ctx.plan(cfgs, graph=False, fft_counts=fft)
+        B, Np, _, _ = plan.execute()
+        plan.close()
+        out.append((B, Np))
+    return out
+
+
+@pytest.mark.parametrize("n_grid,k1,k2,kb", [(64, 4.3, 7.6, 1), (128, 9.1, 13.7, 1), (128, 6.2, 6.2, 2),
+                                             (32, 9.2, 11.4, 1), (48, 8.7, 12.2, 0)])
+def test_enumerated_counts_match_transforms(gpu_lib, ora, n_grid, k1, k2, kb):
+    """Exact pair counts (integer enumeration over orbit representatives,
+    the default for interval shells) equal the FP64 unit-shell transforms'
+    rounded counts, and so do the B they normalise, bit for bit; the 32^3 case
+    (k1 + k2 above N/2 fundamental modes) wraps sums around the grid as the
+    reference's cyclic sums do, and is also checked against the oracle."""
+    ps = gpu_lib
+    box = 150.0
+    kf = 2 * np.pi / box
+    dens, xhii = fields(n_grid, box)
+    dd, xx = field_args(2, dens, xhii)
+    cfgs, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1 * kf, k2=k2 * kf, num_values=7,
+                                            kbinningCase=kb, dcosTheta=0.2)
+    with ps.Context(n_grid, box, methods=ps.PS_FP32_BATCHED) as ctx:
+        ctx.get_FT_field(2, dd, xx, use_only_phase=0)
+        (Be, Ne), (Bf, Nf) = _plan_both_counts(ps, ctx, cfgs)
+    np.testing.assert_array_equal(Ne, Nf)
+    np.testing.assert_array_equal(Be, Bf)
+    if n_grid == 32:
+        p = ora.RunParams(grid_size=n_grid, box_size=box, which_field=2, use_only_phase=0, n=3, equilateral=0,
+                          k1=k1 * kf, k2=k2 * kf, num_values=7, kbinwidth=1.0, kbinning=kb, dcos_theta=0.2)
+        ref = ora.ora_run(p, dd, xx)
+        np.testing.assert_array_equal(Ne, np.rint(ref.npoly))
