@@ -262,6 +262,17 @@ struct ps_gpu_ctx {
     unsigned short* side_lut = nullptr;
     size_t side_lut_cap = 0;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // second field lane: the pair groups of a plan split over two streams (the
+    // main one and this), each with its own FP32 work spectra, partial sums and
+    // shell table, so the kernels of different groups overlap
+    cudaStream_t lane2_stream = nullptr;
+    double* lane2_partials = nullptr;
+    size_t lane2_partials_cap = 0;
+    unsigned short* lane2_lut = nullptr;
+    size_t lane2_lut_cap = 0;
+    V2<float>* lane2_work[3] = {nullptr, nullptr, nullptr};
+    size_t lane2_work_cap = 0;  // elements of each
+    cudaEvent_t ev_join2 = nullptr;
     PrecBufs<float> f;
     PrecBufs<double> d;
     double* partials = nullptr;
@@ -548,6 +559,43 @@ struct SideLane {
         std::swap(c->dlut_cap, c->side_lut_cap);
     }
 };
+
+// While alive, the context's stream, partial sums, shell table and FP32 work
+// spectra are those of the second field lane (not while profiling: then
+// everything runs on the main lane, one launch at a time).
+struct Lane2 {
+    ps_gpu_ctx* c;
+    bool on;
+    explicit Lane2(ps_gpu_ctx* cc, bool always = false) : c(cc), on(always || !cc->prof_on) { swap(); }
+    ~Lane2() { swap(); }
+    void swap()
+    {
+        if (!on) return;
+        std::swap(c->stream, c->lane2_stream);
+        std::swap(c->partials, c->lane2_partials);
+        std::swap(c->partials_cap, c->lane2_partials_cap);
+        std::swap(c->dlut, c->lane2_lut);
+        std::swap(c->dlut_cap, c->lane2_lut_cap);
+        std::swap(c->f.work, c->lane2_work[0]);
+        std::swap(c->f.work2, c->lane2_work[1]);
+        std::swap(c->f.work3, c->lane2_work[2]);
+    }
+};
+
+// FP32 work spectra of the second lane, n elements each (replaced ones are
+// retired: a captured graph may still point at them).
+int ensure_lane2_work(ps_gpu_ctx* c, size_t n)
+{
+    if (n <= c->lane2_work_cap) return PS_OK;
+    for (auto& p : c->lane2_work) {
+        if (p) c->retired.push_back(p);
+        p = nullptr;
+    }
+    c->lane2_work_cap = 0;
+    for (auto& p : c->lane2_work) PS_TRY(alloc_dev(&p, n));
+    c->lane2_work_cap = n;
+    return PS_OK;
+}
 
 int ensure_minmax(ps_gpu_ctx* c, size_t n)
 {
@@ -1880,8 +1928,11 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             return PS_OK;
         });
     }
-    // ---- pair groups
+    // ---- pair groups, split over the main and the second field lane
     bool prefix_done = false;
+    std::vector<std::function<int()>> group_dop(groups.size()), group_iop(groups.size());
+    std::vector<int> group_M(groups.size(), 0);
+    std::vector<size_t> group_need(groups.size(), 0);
     for (size_t g = 0; g < groups.size(); g++) {
         const Group G = groups[g];
         const Shell sa = host_shell_of(G.a), sb = host_shell_of(G.b);
@@ -2000,25 +2051,72 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             PS_TRY(tables_for<float>(c, M, &t32));
             PS_TRY(tables_for<double>(c, M, &t64));
         }
-        if (g == 0) {  // fork the side lane (after the DERIVED chain the counts read)
-            ops.push_back([=]() {
-                PS_CK(cudaEventRecord(c->ev_fork, c->stream));
-                PS_CK(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
-                return PS_OK;
-            });
+        group_dop[g] = d_part(M);
+        group_iop[g] = i_part(M);
+        group_M[g] = M;
+        {   // FP32 work spectra the group's field part writes on its M-grid
+            const int w32 = pw<float>(M);
+            const int s_ab = round_up(std::max(std::min(sa.band, M / 2), std::min(sb.band, M / 2)) + 1, w32);
+            group_need[g] = (size_t)M * M * (size_t)std::max(s_ab, round_up(hout, w32));
         }
-        const auto dop = d_part(M), iop = i_part(M);
+        (void)hsh;
+    }
+    // lanes: the groups by decreasing transform volume, each onto the less
+    // loaded of the main and the second field lane (one lane when profiling
+    // or with a single group)
+    std::vector<int> group_lane(groups.size(), 0);
+    if (groups.size() > 1) {
+        std::vector<size_t> order(groups.size());
+        for (size_t g = 0; g < groups.size(); g++) order[g] = g;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t x, size_t y) { return group_M[x] > group_M[y]; });
+        double load[2] = {0.0, 0.0};
+        size_t need2 = 0;
+        for (size_t g : order) {
+            const int l = load[1] < load[0] ? 1 : 0;
+            group_lane[g] = l;
+            load[l] += (double)group_M[g] * group_M[g] * group_M[g];
+            if (l == 1) need2 = std::max(need2, group_need[g]);
+        }
+        if (need2 > 0) {
+            PS_TRY(ensure_lane2_work(c, need2));
+            const size_t pen32 = (size_t)N * (c->f.S / pw<float>(N));
+            const size_t np = std::max({(size_t)N * N, pen32 * MAX_DOT_SHELLS, (size_t)148 * 8 * 2 * MAX_DOT_SHELLS});
+            Lane2 lane(c, true);  // the second lane's own scratch, profiling or not
+            PS_TRY(ensure_partials(c, np));
+            PS_TRY(ensure_lut(c, (size_t)3 * (N / 2) * (N / 2) + 2));
+        }
+    }
+    if (!groups.empty()) {  // fork the side and second lanes (after the DERIVED chain the groups read)
         ops.push_back([=]() {
-            PS_TRY(dop());
+            PS_CK(cudaEventRecord(c->ev_fork, c->stream));
+            PS_CK(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
+            if (!c->prof_on) PS_CK(cudaStreamWaitEvent(c->lane2_stream, c->ev_fork, 0));
+            return PS_OK;
+        });
+    }
+    for (size_t g = 0; g < groups.size(); g++) {
+        const auto dop = group_dop[g], iop = group_iop[g];
+        const bool second = group_lane[g] == 1;
+        ops.push_back([=]() {
+            if (second) {
+                Lane2 lane(c);
+                PS_TRY(dop());
+            } else {
+                PS_TRY(dop());
+            }
             SideLane lane(c);
             return iop();
         });
-        (void)hsh;
     }
-    if (!groups.empty()) {  // join the side lane
+    if (!groups.empty()) {  // join the side and second lanes
         ops.push_back([=]() {
             PS_CK(cudaEventRecord(c->ev_join, c->side_stream));
             PS_CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+            if (!c->prof_on) {
+                PS_CK(cudaEventRecord(c->ev_join2, c->lane2_stream));
+                PS_CK(cudaStreamWaitEvent(c->stream, c->ev_join2, 0));
+            }
             return PS_OK;
         });
     }
@@ -2695,12 +2793,14 @@ int ps_gpu_create(ps_gpu_ctx** out, int nbins, double boxsize, int methods, int 
             break;
         }
         if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&c->lane2_stream, cudaStreamNonBlocking) != cudaSuccess) {
             rc = fail(PS_ERR_CUDA, "stream creation failed");
             break;
         }
         if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming) != cudaSuccess) {
             rc = fail(PS_ERR_CUDA, "event creation failed");
             break;
         }
@@ -3330,6 +3430,14 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     }
     cudaFree(c->side_partials);
     cudaFree(c->side_lut);
+    if (c->lane2_stream) {
+        cudaStreamSynchronize(c->lane2_stream);
+        cudaStreamDestroy(c->lane2_stream);
+    }
+    cudaFree(c->lane2_partials);
+    cudaFree(c->lane2_lut);
+    for (auto& p : c->lane2_work) cudaFree(p);
+    if (c->ev_join2) cudaEventDestroy(c->ev_join2);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     delete c;
