@@ -145,7 +145,8 @@ template <typename T> struct PrecBufs {
     V2<T>* tw = nullptr;    // W_N^m, m in [0, N): r2c / c2r pre- and post-processing
     V2<T>* twp = nullptr;   // Stockham table of the pencil transforms (length N)
     V2<T>* twr = nullptr;   // Stockham table of the row transforms (length N/2)
-    Tables<T> tables() const { return Tables<T>{twp, twr, tw}; }
+    V2<T>* twp_alt = nullptr;  // table of the alternative Y pass (PencilAlt), if N has one
+    Tables<T> tables() const { return Tables<T>{twp, twr, tw, twp_alt}; }
     V2<T>* spec = nullptr;  // field spectrum, row stride S
     V2<T>* work = nullptr;  // work spectrum (band-limited strides <= S)
     V2<T>* work2 = nullptr; // second and third work spectra (pair groups; allocated on use)
@@ -158,7 +159,7 @@ template <typename T> struct PrecBufs {
     bool have_spec = false;
     bool have_mod = false;
     // tables of smaller transform sizes (sub-grid products), made at plan time
-    std::map<int, std::array<V2<T>*, 3>> sub;
+    std::map<int, std::array<V2<T>*, 4>> sub;
 };
 
 // Host worker threads of the composition, one pool per process shared by
@@ -290,6 +291,9 @@ struct ps_gpu_ctx {
     std::vector<void*> retired;
     // autotuned transform size per pair-group signature (N, b_a, b_b, b_c)
     std::map<std::array<int, 4>, int> tune_grid;
+    // autotuned Y pass geometry per FP32 transform size: 1 = the alternative
+    // (PencilAlt: twice the elements per thread), 0 = the default
+    std::map<int, int> pencil_alt;
     bool capturing = false;  // inside a plan graph capture: no profiling events
     // host uploads: two staging slots of (dens, xhii), filled on copy_stream;
     // ev_copied[s] = slot s filled, ev_free[s] = its forward transform is done
@@ -412,10 +416,16 @@ template <typename T> int init_prec(ps_gpu_ctx* c, PrecBufs<T>& b)
     PS_TRY(alloc_dev(&b.twp, N));
     PS_TRY(alloc_dev(&b.twr, N / 2));
     {
-        std::vector<V2<T>> hp(N), hr(N / 2);
+        std::vector<V2<T>> hp(N), hr(N / 2), ha(N);
         PS_SWITCH_N(N, (L3<T, NN>::host_tables(hp.data(), hr.data())));
         PS_CK(cudaMemcpy(b.twp, hp.data(), sizeof(V2<T>) * N, cudaMemcpyHostToDevice));
         PS_CK(cudaMemcpy(b.twr, hr.data(), sizeof(V2<T>) * (N / 2), cudaMemcpyHostToDevice));
+        bool has_alt = false;
+        PS_SWITCH_N(N, (has_alt = L3<T, NN>::host_alt_table(ha.data())));
+        if (has_alt) {
+            PS_TRY(alloc_dev(&b.twp_alt, N));
+            PS_CK(cudaMemcpy(b.twp_alt, ha.data(), sizeof(V2<T>) * N, cudaMemcpyHostToDevice));
+        }
     }
     PS_TRY(alloc_dev(&b.spec, nspec));
     PS_TRY(alloc_dev(&b.work, nspec));
@@ -446,10 +456,12 @@ template <typename T> int tables_for(ps_gpu_ctx* c, int M, Tables<T>* out)
     auto it = b.sub.find(M);
     if (it == b.sub.end()) {
         if (c->capturing) return fail(PS_ERR_ARG, "internal: tables of size %d not made before capture", M);
-        std::array<V2<T>*, 3> t = {nullptr, nullptr, nullptr};
-        std::vector<V2<T>> hp(M), hr(M / 2), h(M);
+        std::array<V2<T>*, 4> t = {nullptr, nullptr, nullptr, nullptr};
+        std::vector<V2<T>> hp(M), hr(M / 2), h(M), ha(M);
         const int N = M;
         PS_SWITCH_N(N, (L3<T, NN>::host_tables(hp.data(), hr.data())));
+        bool has_alt = false;
+        PS_SWITCH_N(N, (has_alt = L3<T, NN>::host_alt_table(ha.data())));
         const long double two_pi = 6.283185307179586476925286766559005768L;
         for (int m = 0; m < M; m++) {
             const long double a = two_pi * (long double)m / (long double)M;
@@ -459,6 +471,7 @@ template <typename T> int tables_for(ps_gpu_ctx* c, int M, Tables<T>* out)
         int rc = alloc_dev(&t[0], M);
         if (rc == PS_OK) rc = alloc_dev(&t[1], M / 2);
         if (rc == PS_OK) rc = alloc_dev(&t[2], M);
+        if (rc == PS_OK && has_alt) rc = alloc_dev(&t[3], M);
         if (rc != PS_OK) {
             for (V2<T>* p : t) cudaFree(p);
             return rc;
@@ -467,9 +480,10 @@ template <typename T> int tables_for(ps_gpu_ctx* c, int M, Tables<T>* out)
         PS_CK(cudaMemcpy(t[0], hp.data(), sizeof(V2<T>) * M, cudaMemcpyHostToDevice));
         PS_CK(cudaMemcpy(t[1], hr.data(), sizeof(V2<T>) * (M / 2), cudaMemcpyHostToDevice));
         PS_CK(cudaMemcpy(t[2], h.data(), sizeof(V2<T>) * M, cudaMemcpyHostToDevice));
+        if (has_alt) PS_CK(cudaMemcpy(t[3], ha.data(), sizeof(V2<T>) * M, cudaMemcpyHostToDevice));
         it = b.sub.find(M);
     }
-    *out = Tables<T>{it->second[0], it->second[1], it->second[2]};
+    *out = Tables<T>{it->second[0], it->second[1], it->second[2], it->second[3]};
     return PS_OK;
 }
 
@@ -481,6 +495,7 @@ template <typename T> void free_prec(PrecBufs<T>& b)
     cudaFree(b.tw);
     cudaFree(b.twp);
     cudaFree(b.twr);
+    cudaFree(b.twp_alt);
     cudaFree(b.spec);
     cudaFree(b.work);
     cudaFree(b.work2);
@@ -615,6 +630,14 @@ template <typename T> PrecBufs<T>& bufs(ps_gpu_ctx* c);
 template <> PrecBufs<float>& bufs<float>(ps_gpu_ctx* c) { return c->f; }
 template <> PrecBufs<double>& bufs<double>(ps_gpu_ctx* c) { return c->d; }
 
+// Y pass geometry of an M-point transform of precision T (autotuned choice).
+template <typename T> int pencil_alt_of(const ps_gpu_ctx* c, int M)
+{
+    if (sizeof(T) != 4) return 0;
+    const auto it = c->pencil_alt.find(M);
+    return it == c->pencil_alt.end() ? 0 : it->second;
+}
+
 }  // namespace
 
 int ps::launch_fail(cudaError_t e, const char* what)
@@ -722,7 +745,8 @@ int c2r_xy(ps_gpu_ctx* c, int mode, const Shell* dshell, int band, V2<T>* dst, i
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, tb, quad, std::min(band, N / 2)))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, dst, S, true, tb, quad, std::min(band, N / 2), 0, NN,
+                                                 pencil_alt_of<T>(c, N)))));
         const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
         pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V, N);
     }
@@ -780,7 +804,8 @@ int pair_spectrum(ps_gpu_ctx* c, const V2<T>* A, int Sa, int hba, const V2<T>* B
     {
         Prof pf(c);
         // rows |my| >= hout lie outside every shell the product is dotted with
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, tb, quad, NN, 0, hout - 1))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.work3, S, false, tb, quad, NN, 0, hout - 1,
+                                                 pencil_alt_of<T>(c, N)))));
         pf.end(fam<T>(KF_PASS_Y), 2.0 * q * NN2 * S * V, N);
     }
     *S_out = S;
@@ -1541,6 +1566,56 @@ int tune_grid(ps_gpu_ctx* c, const std::function<std::function<int()>(int)>& gro
     return rc;
 }
 
+// Autotuning of the FP32 Y pass geometry of an M-point transform: the
+// default and the alternative (PencilAlt) each run once to warm up, then
+// three times timed with CUDA events, in place on a scratch work spectrum of
+// M planes of band-limited width; the faster is kept for the context.
+int tune_pencil(ps_gpu_ctx* c, int M)
+{
+    if (c->pencil_alt.count(M)) return PS_OK;
+    bool has_alt = false;
+    {
+        const int N = M;
+        PS_SWITCH_N(N, (has_alt = L3<float, NN>::ALT > 0));
+    }
+    if (!has_alt || !c->f.work) {
+        c->pencil_alt[M] = 0;
+        return PS_OK;
+    }
+    Tables<float> tb;
+    PS_TRY(tables_for<float>(c, M, &tb));
+    const int S = std::min(c->f.S, round_up(M / 2 + 1, pw<float>(M)));
+    if ((size_t)M * M * S > (size_t)c->N * c->N * c->f.S) {
+        c->pencil_alt[M] = 0;
+        return PS_OK;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PS_CK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(PS_ERR_CUDA, "event creation failed");
+    }
+    float ms[2] = {0.f, 0.f};
+    int rc = PS_OK;
+    for (int alt = 0; alt < 2 && rc == PS_OK; alt++) {
+        const int N = M;
+        auto run = [&]() -> int {
+            PS_SWITCH_N(N, PS_TRY((L3<float, NN>::pass_y(c->stream, c->f.work, S, true, tb, 0, NN, 0, NN, alt))));
+            return PS_OK;
+        };
+        if ((rc = run()) != PS_OK) break;
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 3 && rc == PS_OK; r++) rc = run();
+        cudaEventRecord(e1, c->stream);
+        if (rc == PS_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = fail(PS_ERR_CUDA, "autotune timing failed");
+        if (rc == PS_OK) cudaEventElapsedTime(&ms[alt], e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == PS_OK) c->pencil_alt[M] = ms[1] < ms[0] ? 1 : 0;
+    return rc;
+}
+
 int sum_partials_n(ps_gpu_ctx* c, int nblocks, int ncols, double* out)
 {
     return sum_partials(c, nblocks, ncols, out, 1);
@@ -2060,6 +2135,9 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             group_need[g] = (size_t)M * M * (size_t)std::max(s_ab, round_up(hout, w32));
         }
         (void)hsh;
+    }
+    if (P->flags & PS_PLAN_AUTOTUNE) {  // the FP32 Y pass geometry of the pair groups' transform sizes
+        for (size_t g = 0; g < groups.size(); g++) PS_TRY(tune_pencil(c, group_M[g]));
     }
     // lanes: the groups by decreasing transform volume, each onto the less
     // loaded of the main and the second field lane (one lane when profiling
@@ -3318,6 +3396,10 @@ int ps_gpu_tune_export(ps_gpu_ctx* c, char* buf, int buflen)
                  kv.second);
         t += line;
     }
+    for (const auto& kv : c->pencil_alt) {
+        snprintf(line, sizeof(line), "pencil %d %d\n", kv.first, kv.second);
+        t += line;
+    }
     if (buf && buflen > 0) {
         const size_t n = std::min(t.size(), (size_t)buflen - 1);
         memcpy(buf, t.data(), n);
@@ -3331,6 +3413,7 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
     g_err[0] = 0;
     if (!c || !text) return fail(PS_ERR_ARG, "NULL argument");
     std::map<std::array<int, 4>, int> add;
+    std::map<int, int> add_pencil;
     const char* p = text;
     while (*p) {
         const char* e = strchr(p, '\n');
@@ -3338,6 +3421,14 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
         p = e ? e + 1 : p + ln.size();
         if (ln.find_first_not_of(" \t\r") == std::string::npos) continue;
         int n, ba, bb, bc, m, used = 0;
+        if (sscanf(ln.c_str(), "pencil %d %d %n", &m, &n, &used) == 2 &&
+            ln.find_first_not_of(" \t\r", used) == std::string::npos) {
+            if (!grid_size_ok(m) || (n != 0 && n != 1))
+                return fail(PS_ERR_ARG, "tune line out of range: '%s'", ln.c_str());
+            add_pencil[m] = n;
+            continue;
+        }
+        used = 0;
         if (sscanf(ln.c_str(), "grid %d %d %d %d %d %n", &n, &ba, &bb, &bc, &m, &used) != 5 ||
             ln.find_first_not_of(" \t\r", used) != std::string::npos)
             return fail(PS_ERR_ARG, "tune line not understood: '%s'", ln.c_str());
@@ -3346,6 +3437,7 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
         add[{n, ba, bb, bc}] = m;
     }
     for (const auto& kv : add) c->tune_grid[kv.first] = kv.second;
+    for (const auto& kv : add_pencil) c->pencil_alt[kv.first] = kv.second;
     return PS_OK;
 }
 

@@ -68,6 +68,39 @@ template <int M> Tables<float> make_tables()
 }
 static int rup(int a, int b) { return (a + b - 1) / b * b; }
 
+// Mean time of `reps` launches of the Y pass variant <M, INV, RX> over the
+// pencils of data (stride S, ncols columns, input rows |my| <= jband, output
+// rows |my| <= jout), with its own Stockham table.
+template <int M, bool INV, int RX>
+double time_pass_y(int reps, float2* data, int S, int ncols, int jband, int jout, const char* what)
+{
+    using G = PencilGeom<float, M, RX>;
+    std::vector<float2> hp(M);
+    transform_table<float2, M, G::R, G::TPF>(hp.data());
+    float2* tw;
+    CK(cudaMalloc(&tw, M * 8));
+    CK(cudaMemcpy(tw, hp.data(), M * 8, cudaMemcpyHostToDevice));
+    auto kern = k_pass_y<float, M, INV, RX>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::THREADS, G::SMEM));
+    const unsigned blocks = (unsigned)(M * (ncols / G::W));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int it = 0; it < 3; it++) kern<<<blocks, G::THREADS, G::SMEM>>>(data, S, ncols, 0, jband, jout, tw);
+    CK(cudaEventRecord(e0));
+    for (int it = 0; it < reps; it++) kern<<<blocks, G::THREADS, G::SMEM>>>(data, S, ncols, 0, jband, jout, tw);
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    printf("pass_y %s@%d R=%d: %.4f ms  (%d threads, %d CTAs/SM)\n", what, M, G::R, ms / reps, G::THREADS, per_sm);
+    CK(cudaFree(tw));
+    return ms / reps;
+}
+
 // Row Stockham table of the pair kernel variant <M, RX>.
 template <int M, int RX> float2* pair_row_table()
 {
@@ -180,6 +213,15 @@ int main(int argc, char** argv)
     }
     CK(cudaDeviceSynchronize());
     for (int q = 0; q < NK; q++) printf("%-18s %.4f ms\n", names[q], tm.acc[q] / reps);
+
+    // Y pass variants (elements per thread: the default and twice it)
+    time_pass_y<384, true, 0>(reps, wb, Sb, Sb, bb, M, "inv B");
+    time_pass_y<384, true, 24>(reps, wb, Sb, Sb, bb, M, "inv B");
+    time_pass_y<384, false, 0>(reps, w3, S, S, M, bc, "fwd");
+    time_pass_y<384, false, 24>(reps, w3, S, S, M, bc, "fwd");
+    time_pass_y<512, false, 0>(reps, spec, SN, 176, N, N, "field");
+    time_pass_y<512, false, 32>(reps, spec, SN, 176, N, N, "field");
+    time_pass_y<512, false, 8>(reps, spec, SN, 176, N, N, "field");
 
     // pair kernel variants: the 384-point group above, and a 320-point group
     // (leg bands 52 and 77, closing band 128: the shapes of the third sweep)

@@ -40,8 +40,10 @@ template <typename T, int N> struct PencilThreads {
     static constexpr int value = LenKind<N>::RAGGED ? ((sizeof(T) == 8 && N > 512) ? 64 : LenKind<N>::RAGGED_TPF)
                                : N / ((sizeof(T) == 4 && N == 512) ? 16 : DefaultRadix<N>::value);
 };
-template <typename T, int N> struct PencilGeom {
-    static constexpr int TPF = PencilThreads<T, N>::value;
+// RX > 0 overrides the elements per thread of a register-plan pencil length
+// (pass variants with fewer, larger radix passes).
+template <typename T, int N, int RX = 0> struct PencilGeom {
+    static constexpr int TPF = RX > 0 && !LenKind<N>::RAGGED ? N / RX : PencilThreads<T, N>::value;
     static constexpr int R = (N + TPF - 1) / TPF;
     // element e of thread t is position t + TPF e of the transform; with
     // R * TPF > N (ragged lengths) the positions past N are idle slots
@@ -59,6 +61,14 @@ template <typename T, int N> struct PencilGeom {
     static constexpr size_t DK_BYTES = (size_t)N * W * sizeof(V2<T>);
     static constexpr bool DK_SMEM = sizeof(T) == 4 && SMEM + DK_BYTES <= 227 * 1024;
     static constexpr size_t SMEM_DOT = SMEM + (DK_SMEM ? DK_BYTES : 0);
+};
+
+// The alternative pencil geometry of the FP32 Y pass for the larger
+// register-plan lengths: twice the elements per thread, half the threads per
+// pencil, one radix pass fewer (0: none).  Chosen per length by the plan
+// autotuner against the default.
+template <typename T, int N> struct PencilAlt {
+    static constexpr int value = (sizeof(T) == 4 && !LenKind<N>::RAGGED && N >= 128 && N <= 512) ? 2 * PencilGeom<T, N>::R : 0;
 };
 
 // Elements per thread of the row (contiguous-axis) transforms of length NH:
@@ -257,12 +267,12 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
 }
 
 // ------------------------------------------------------------------ Y pass
-template <typename T, int N, bool INV>
-__global__ void __launch_bounds__(PencilGeom<T, N>::THREADS)
+template <typename T, int N, bool INV, int RX = 0>
+__global__ void __launch_bounds__(PencilGeom<T, N, RX>::THREADS)
     k_pass_y(V2<T>* __restrict__ data, int stride, int ncols, int quad, int jband, int jout,
              const V2<T>* __restrict__ tw_g)
 {
-    using G = PencilGeom<T, N>;
+    using G = PencilGeom<T, N, RX>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;

@@ -58,6 +58,7 @@ template <typename T> struct Tables {
     const V2<T>* twp;
     const V2<T>* twr;
     const V2<T>* twpp;
+    const V2<T>* twp_alt = nullptr;  // Stockham table of the alternative Y pass (PencilAlt), if any
 };
 
 template <typename T, int N> struct L3 {
@@ -65,6 +66,19 @@ template <typename T, int N> struct L3 {
     using PG = PencilGeom<T, N>;
     using RG = RowGeom<T, N>;
     static int pencil_width() { return PG::W; }
+    static constexpr int ALT = PencilAlt<T, N>::value;
+    // host copy of the alternative Y pass's table (false: no alternative)
+    static bool host_alt_table(V* twp_alt)
+    {
+        if constexpr (ALT > 0) {
+            static_assert(PencilGeom<T, N, ALT>::W == PG::W, "same pencil tile width");
+            transform_table<V, N, ALT, PencilGeom<T, N, ALT>::TPF>(twp_alt);
+            return true;
+        } else {
+            (void)twp_alt;
+            return false;
+        }
+    }
     // host copies of the tables for this N
     static void host_tables(V* twp, V* twr)
     {
@@ -88,12 +102,28 @@ template <typename T, int N> struct L3 {
     // jband < N/2: input rows with |my| > jband are zero and are not read
     // ncols (0: stride): only columns h < ncols, a multiple of the pencil width
     // jout < N/2: output rows with |my| > jout are not stored
+    // alt: the alternative geometry (PencilAlt) when this length has one
     static int pass_y(cudaStream_t st, V* data, int stride, bool inv, const Tables<T>& tb, int quad = 0,
-                      int jband = N, int ncols = 0, int jout = N)
+                      int jband = N, int ncols = 0, int jout = N, int alt = 0)
     {
         const int ni = quad ? N / 2 + 1 : N;
         const int nc = ncols > 0 ? ncols : stride;
         const unsigned blocks = (unsigned)(ni * (nc / PG::W));
+        if constexpr (ALT > 0) {
+            if (alt && tb.twp_alt) {
+                using PA = PencilGeom<T, N, ALT>;
+                if (inv) {
+                    PS_LTRY(set_smem(k_pass_y<T, N, true, ALT>, PA::SMEM));
+                    k_pass_y<T, N, true, ALT><<<blocks, PA::THREADS, PA::SMEM, st>>>(data, stride, nc, quad, jband, jout,
+                                                                                     tb.twp_alt);
+                } else {
+                    PS_LTRY(set_smem(k_pass_y<T, N, false, ALT>, PA::SMEM));
+                    k_pass_y<T, N, false, ALT><<<blocks, PA::THREADS, PA::SMEM, st>>>(data, stride, nc, quad, jband,
+                                                                                      jout, tb.twp_alt);
+                }
+                return PS_OK;
+            }
+        }
         if (inv) {
             PS_LTRY(set_smem(k_pass_y<T, N, true>, PG::SMEM));
             k_pass_y<T, N, true><<<blocks, PG::THREADS, PG::SMEM, st>>>(data, stride, nc, quad, jband, jout, tb.twp);

@@ -319,7 +319,8 @@ def test_mixed_radix_subgrids_match_plain(gpu_lib, n_grid, pairs):
 
 
 def test_autotuned_plan_and_tune_table(gpu_lib):
-    """An autotuned plan (transform size per pair group picked by timing) keeps
+    """An autotuned plan (transform size per pair group and Y pass geometry
+    per transform size picked by timing) keeps
     counts and derived ranges identical and B within the batched tolerance of
     plain FP64; its choices exported from one context and imported into
     another reproduce its results bit for bit without timing."""
@@ -339,6 +340,7 @@ def test_autotuned_plan_and_tune_table(gpu_lib):
         B64, N64, _, out64 = ctx.batch(cfgs, ps.PS_FP64_PLAIN)
         table = ctx.tune_export()
     assert table.count("grid ") >= 2, table
+    assert "pencil " in table, table  # the Y pass geometry per transform size
     scale = np.abs(B64).max()
     assert np.all(np.abs(Bt - B64) <= 1e-5 * np.abs(B64) + 1e-6 * scale)
     np.testing.assert_array_equal(Nt, np.rint(N64))
