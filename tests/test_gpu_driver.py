@@ -104,3 +104,19 @@ def test_driver_exact_sidecar(gpu_lib, ref_exe, tmp_path):
         legs = np.array(e[2:-2]).reshape(3, 3)
         np.testing.assert_array_equal(legs[:, 1], list(out[i].kmin)[:3])
         np.testing.assert_array_equal(legs[:, 2], list(out[i].kmax)[:3])
+
+
+def test_driver_prints_condition_numbers(tmp_path, gpu_lib):
+    """Per configuration, ps_run prints the condition number of the value sum
+    where the reference prints the imaginary over the real part of its sums
+    (polyspectrum.c:142); --no-kappa leaves those lines out."""
+    from _driver import make_run, run_driver
+    ini = make_run(str(tmp_path), kbinning=1, phase=1)
+    out = run_driver(ini, cwd=str(tmp_path), timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("rank 0: kappa(sumValuesPolygons) = ")]
+    assert len(lines) == 4, out.stdout
+    for ln in lines:
+        assert float(ln.split("=")[1].split()[0]) >= 1.0
+    out2 = run_driver(ini, "--no-kappa", cwd=str(tmp_path), timeout=300)
+    assert out2.returncode == 0 and "kappa" not in out2.stdout, out2.stdout
