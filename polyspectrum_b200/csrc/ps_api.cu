@@ -872,8 +872,11 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     }
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tables(), 0, NN, ncols))));
-        pf.end(fam<T>(KF_PASS_Y), 2.0 * NN2 * ncols * V, N);
+        // rows |my| > band are read by no later pass: not stored
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pass_y(c->stream, B.spec, B.S, false, B.tables(), 0, NN, ncols,
+                                                 band < N / 2 ? band : NN))));
+        const double rows_out = band < N / 2 ? (double)N * (2 * band + 1) : NN2;
+        pf.end(fam<T>(KF_PASS_Y), (NN2 + rows_out) * ncols * V, N);
     }
     {
         Prof pf(c);
