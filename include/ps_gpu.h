@@ -347,8 +347,10 @@ int ps_gpu_power_spectrum_noalloc(int nbins, double boxsize, const float *field_
  * utils.c:96).  spec "alloc:N", "read:N" or "launch:N" (comma-separated to arm
  * several): the Nth device or page-locked allocation, input-file read or
  * post-launch status check after this call fails once, with the status a
- * real failure returns (PS_ERR_OOM, PS_ERR_IO, PS_ERR_CUDA); no GPU fault is
- * caused.  NULL or "" disarms.  $PS_FAULT arms the same way at the process's
+ * real failure returns (PS_ERR_OOM, PS_ERR_IO, PS_ERR_CUDA); "wait:N": the Nth
+ * field transform staged by bulk copies waits on a barrier that cannot
+ * complete, so its bounded wait (0.2 s) runs out and the load returns
+ * PS_ERR_TIMEOUT.  No GPU fault is caused.  NULL or "" disarms.  $PS_FAULT arms the same way at the process's
  * first ps_gpu_create.  Malformed spec: PS_ERR_ARG. */
 int ps_gpu_debug_fault(const char *spec);
 

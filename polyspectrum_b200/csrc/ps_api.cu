@@ -49,9 +49,12 @@ int fail(int code, const char* fmt, ...)
 // ever caused): once armed with "alloc:N", "read:N" or "launch:N" (a comma
 // separated list arms several), the Nth device or page-locked allocation,
 // input-file read or post-launch status check after arming fails once, with
-// the status the real failure returns (PS_ERR_OOM, PS_ERR_IO, PS_ERR_CUDA).
+// the status the real failure returns (PS_ERR_OOM, PS_ERR_IO, PS_ERR_CUDA);
+// "wait:N" makes the Nth bulk-staged field transform's mbarrier expect 16
+// bytes more than its copies bring, so its bounded wait runs out and the load
+// returns PS_ERR_TIMEOUT (the copies themselves complete).
 // Armed by ps_gpu_debug_fault, or by $PS_FAULT at the first ps_gpu_create.
-enum FaultKind { FAULT_ALLOC = 0, FAULT_READ = 1, FAULT_LAUNCH = 2, FAULT_KINDS = 3 };
+enum FaultKind { FAULT_ALLOC = 0, FAULT_READ = 1, FAULT_LAUNCH = 2, FAULT_WAIT = 3, FAULT_KINDS = 4 };
 std::atomic<long long> g_fault_at[FAULT_KINDS];
 std::atomic<long long> g_fault_seen[FAULT_KINDS];
 
@@ -66,8 +69,8 @@ bool fault_hit(int kind)
 
 int arm_faults(const char* spec)
 {
-    long long at[FAULT_KINDS] = {0, 0, 0};
-    static const char* names[FAULT_KINDS] = {"alloc", "read", "launch"};
+    long long at[FAULT_KINDS] = {0, 0, 0, 0};
+    static const char* names[FAULT_KINDS] = {"alloc", "read", "launch", "wait"};
     if (spec && *spec) {
         std::string txt(spec);
         size_t pos = 0;
@@ -81,8 +84,8 @@ int arm_faults(const char* spec)
                 if (item.compare(0, colon, names[q]) == 0 && colon == strlen(names[q])) kind = q;
             char* tail = nullptr;
             const long long n = kind >= 0 ? strtoll(item.c_str() + colon + 1, &tail, 10) : 0;
-            if (kind < 0 || n <= 0 || !tail || *tail) return fail(PS_ERR_ARG, "fault spec '%s': want alloc:N, read:N "
-                                                                               "or launch:N, N >= 1", item.c_str());
+            if (kind < 0 || n <= 0 || !tail || *tail) return fail(PS_ERR_ARG, "fault spec '%s': want alloc:N, read:N, "
+                                                                               "launch:N or wait:N, N >= 1", item.c_str());
             at[kind] = n;
             pos = end + 1;
         }
@@ -329,6 +332,7 @@ struct ps_gpu_ctx {
     std::map<std::string, double> npoly_cache;
     cudaEvent_t ev_raw[2] = {nullptr, nullptr};
     std::atomic<int> async_err{0};  // status of submissions unpacked after their call returned
+    int* dstatus = nullptr;  // device word: 1 when a kernel's bounded wait expired (PS_ERR_TIMEOUT)
     std::set<ps_gpu_plan*> plans;   // live plans (finalize releases their device memory)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
@@ -859,14 +863,17 @@ template <typename T> int forward_field(ps_gpu_ctx* c, int kind, const void* a, 
     {
         Prof pf(c);
         if (split == 0) {
-            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, hcols, B.tables()))));
+            const int extra = fault_hit(FAULT_WAIT) ? 16 : 0;
+            PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, kind, a, b, B.spec, B.S, hcols, B.tables(), -1, 0,
+                                                    c->dstatus, extra))));
         } else {
             const size_t nr = (size_t)N * N;
             const float* af = (const float*)a;
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, SRC_XHI_F32, af, b, B.spec, B.S, hcols, B.tables(),
-                                                    -1, split))));
+                                                    -1, split, c->dstatus))));
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_z(c->stream, SRC_F32, af + split * N, nullptr,
-                                                    B.spec + split * B.S, B.S, hcols, B.tables(), -1, nr - split))));
+                                                    B.spec + split * B.S, B.S, hcols, B.tables(), -1, nr - split,
+                                                    c->dstatus))));
         }
         pf.end(fam<T>(KF_FWD_Z), NN2 * N * src_bytes + NN2 * H * V, N);
     }
@@ -2560,6 +2567,22 @@ int grad_impl(ps_gpu_ctx* c, int n, const std::vector<Shell>& legs, double scale
     return PS_OK;
 }
 
+// PS_ERR_TIMEOUT (and the word cleared) when a kernel's bounded wait on this
+// context's stream expired; call after the stream work it covers is done.
+int check_status(ps_gpu_ctx* c)
+{
+    int h = 0;
+    PS_CK(cudaMemcpyAsync(&h, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PS_CK(cudaStreamSynchronize(c->stream));
+    if (h) {
+        PS_CK(cudaMemsetAsync(c->dstatus, 0, sizeof(int), c->stream));
+        c->f.have_spec = c->d.have_spec = false;  // the field spectrum is incomplete
+        c->field_set = false;
+        return fail(PS_ERR_TIMEOUT, "a bulk copy into shared memory did not complete within its wait limit");
+    }
+    return PS_OK;
+}
+
 int timed_begin(ps_gpu_ctx* c)
 {
     c->launches = 0;
@@ -2893,6 +2916,11 @@ int ps_gpu_create(ps_gpu_ctx** out, int nbins, double boxsize, int methods, int 
             rc = fail(PS_ERR_CUDA, "event creation failed");
             break;
         }
+        if ((rc = alloc_dev(&c->dstatus, 1)) != PS_OK) break;
+        if (cudaMemset(c->dstatus, 0, sizeof(int)) != cudaSuccess) {
+            rc = fail(PS_ERR_CUDA, "status word");
+            break;
+        }
         // the batched method transforms shells in FP32 and counts in FP64
         if (methods & PS_FP32_BATCHED) {
             if ((rc = init_prec(c, c->f)) != PS_OK) break;
@@ -2916,7 +2944,8 @@ int ps_gpu_set_field(ps_gpu_ctx* c, int which, const void* dens, const void* xhi
     PS_CK(cudaSetDevice(c->device));
     PS_TRY(timed_begin(c));
     PS_TRY(load_field(c, which, dens, xhii, is_double, mem, use_only_phase));
-    return timed_end(c);
+    PS_TRY(timed_end(c));
+    return check_status(c);
 }
 
 int ps_gpu_set_field_async(ps_gpu_ctx* c, int which, const void* dens, const void* xhii, int is_double,
@@ -3006,7 +3035,8 @@ int ps_gpu_set_field_files(ps_gpu_ctx* c, int which, const char* dens_path, int 
     PS_CK(cudaStreamWaitEvent(c->stream, c->ev_copied[s], 0));
     PS_TRY(transform_field(c, c->stage[s][0], nin > 1 ? c->stage[s][1] : nullptr, dp, use_only_phase, s));
     PS_CK(cudaStreamSynchronize(c->copy_stream));
-    return timed_end(c);
+    PS_TRY(timed_end(c));
+    return check_status(c);
 }
 
 int ps_gpu_init(ps_gpu_ctx** ctx, int nbins, double boxsize, const void* field, int field_is_double,
@@ -3357,6 +3387,7 @@ int ps_gpu_synchronize(ps_gpu_ctx* c)
     PS_CK(cudaStreamSynchronize(c->copy_stream));
     PS_CK(cudaStreamSynchronize(c->stream));
     PS_TRY(drain_pending(c, true));
+    PS_TRY(check_status(c));
     const int e = c->async_err.exchange(0);
     if (e != PS_OK) return fail(e, "internal: a derived shell exceeded its launch bound (asynchronous execution)");
     return PS_OK;
@@ -3499,6 +3530,7 @@ void ps_gpu_finalize(ps_gpu_ctx* c)
     free_prec(c->f);
     free_prec(c->d);
     cudaFree(c->partials);
+    cudaFree(c->dstatus);
     cudaFree(c->dsums);
     cudaFree(c->dshells);
     cudaFree(c->dminmax);

@@ -188,14 +188,18 @@ int main(int argc, char** argv)
     Tables<float> T5 = make_tables<512>(), T3 = make_tables<384>();
     using L5 = L3<float, 512>;
     using L4 = L3<float, 384>;
-    const char* names[] = {"fwd_z@512 direct", "fwd_z@512 staged", "pass_y@512", "fwd_x_store@512", "inv_x A@384", "pass_y A@384", "inv_x B@384",
+    const char* names[] = {"fwd_z@512 direct", "fwd_z@512 staged", "fwd_z@512 bulk", "pass_y@512", "fwd_x_store@512", "inv_x A@384", "pass_y A@384", "inv_x B@384",
                            "pass_y B@384", "pair_z@384", "pass_y fwd@384", "fwd_x_dot@384"};
-    const int NK = 11;
+    const int NK = 12;
+    int* status;
+    CK(cudaMalloc(&status, sizeof(int)));
+    CK(cudaMemset(status, 0, sizeof(int)));
     Timer tm(NK);
     for (int it = 0; it < reps + 3; it++) {
         tm.start();
         LT(L5::fwd_z(0, SRC_XHI_F32, da, db, spec, SN, hcols, T5, 0)); tm.lap();
         LT(L5::fwd_z(0, SRC_XHI_F32, da, db, spec, SN, hcols, T5, 1)); tm.lap();
+        LT(L5::fwd_z(0, SRC_XHI_F32, da, db, spec, SN, hcols, T5, 1, 0, status)); tm.lap();
         LT(L5::pass_y(0, spec, SN, false, T5, 0, N, 176)); tm.lap();
         LT(L5::fwd_x(0, spec, SN, hcols, SPEC_STORE_PHASE, spec, SN, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, T5,
                      nullptr, 1.0, 0, 0, 0x7fffffff, nullptr, 176, 164)); tm.lap();
@@ -213,6 +217,9 @@ int main(int argc, char** argv)
     }
     CK(cudaDeviceSynchronize());
     for (int q = 0; q < NK; q++) printf("%-18s %.4f ms\n", names[q], tm.acc[q] / reps);
+    int hstatus = 0;
+    CK(cudaMemcpy(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hstatus) { fprintf(stderr, "bulk copy wait expired\n"); return 1; }
 
     // Y pass variants (elements per thread: the default and twice it)
     time_pass_y<384, true, 0>(reps, wb, Sb, Sb, bb, M, "inv B");

@@ -532,15 +532,42 @@ __device__ __forceinline__ V2<T> load_pair(int kind, const unsigned char* ra, co
 //    loader reads its value pairs from there, so no register holds a load in
 //    flight; FP32 rows of 512 then run four 256-thread CTAs per SM with up to
 //    64 registers.  Needs 16-byte aligned inputs of 4- or 8-byte values.
+//    With BULK the tile arrives by one bulk copy per input array
+//    (cp.async.bulk through the TMA engine, completion counted on an mbarrier)
+//    instead of one 16-byte cp.async per thread and chunk.  The wait on the
+//    mbarrier is bounded (kBulkWaitNs of the global timer): past the limit the
+//    kernel sets *status to 1, waits once more (bounded) for the copies and
+//    returns without writing.  tx_extra > 0 (fault injection in tests) makes
+//    the barrier expect more bytes than the copies bring, so the wait runs out.
 //  * direct: all loads issued up front into registers (`vec`: one vector load
 //    per value pair); FP32 rows of 512 are held to 32 registers so that eight
 //    CTAs (every warp slot of the SM) keep their loads in flight.
-template <typename T, int N, bool STAGED>
+constexpr unsigned long long kBulkWaitNs = 200000000ull;  // 0.2 s before a bulk copy counts as lost
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool mbar_try_wait_parity(unsigned bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return done != 0u;
+}
+
+template <typename T, int N, bool STAGED, bool BULK = false>
 __global__ void __launch_bounds__(RowGeom<T, N>::THREADS,
                                   (sizeof(T) == 4 && N == 512) ? (STAGED ? 4 : 8) : 1)
     k_fwd_z(int kind, const void* __restrict__ a_src, const void* __restrict__ b_src,
             V2<T>* __restrict__ dst, int dst_stride, int hout, int vec, const V2<T>* __restrict__ twr_g,
-            const V2<T>* __restrict__ twpp_g)
+            const V2<T>* __restrict__ twpp_g, int* __restrict__ status = nullptr, int tx_extra = 0)
 {
     using G = RowGeom<T, N>;
     using V = V2<T>;
@@ -556,13 +583,48 @@ __global__ void __launch_bounds__(RowGeom<T, N>::THREADS,
         const unsigned char* ga = reinterpret_cast<const unsigned char*>(a_src) + (size_t)blockIdx.x * tile_bytes;
         const unsigned char* gb =
             b_src ? reinterpret_cast<const unsigned char*>(b_src) + (size_t)blockIdx.x * tile_bytes : nullptr;
-        for (size_t c = threadIdx.x; c < tile_bytes / 16; c += G::THREADS) {
-            cp_async16(sa + 16 * c, ga + 16 * c);
-            if (gb) cp_async16(sb + 16 * c, gb + 16 * c);
+        __shared__ __align__(8) unsigned long long bar;  // BULK: completion of the tile's copies
+        const unsigned bar_s = (unsigned)__cvta_generic_to_shared(&bar);
+        if constexpr (BULK) {
+            if (threadIdx.x == 0) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_s) : "memory");
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const unsigned bytes = (unsigned)tile_bytes, total = bytes * (gb ? 2u : 1u) + (unsigned)tx_extra;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_s), "r"(total)
+                             : "memory");
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             ::"r"((unsigned)__cvta_generic_to_shared(sa)), "l"(ga), "r"(bytes), "r"(bar_s)
+                             : "memory");
+                if (gb)
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                        ::"r"((unsigned)__cvta_generic_to_shared(sb)), "l"(gb), "r"(bytes), "r"(bar_s)
+                        : "memory");
+            }
+        } else {
+            for (size_t c = threadIdx.x; c < tile_bytes / 16; c += G::THREADS) {
+                cp_async16(sa + 16 * c, ga + 16 * c);
+                if (gb) cp_async16(sb + 16 * c, gb + 16 * c);
+            }
+            cp_async_commit();
         }
-        cp_async_commit();
-        RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);
-        cp_async_wait_all();
+        RowCtx<T, N> rc(smem_raw, twr_g, twpp_g);  // tables staged while the copies fly
+        if constexpr (BULK) {
+            bool arrived = mbar_try_wait_parity(bar_s, 0u);
+            for (const unsigned long long t0 = global_ns(); !arrived && global_ns() - t0 < kBulkWaitNs;)
+                arrived = mbar_try_wait_parity(bar_s, 0u);
+            if (!__syncthreads_and(arrived)) {  // the copy never completed: report, wait once more, leave
+                if (threadIdx.x == 0 && status) atomicExch(status, 1);
+                for (const unsigned long long t0 = global_ns(); !arrived && global_ns() - t0 < kBulkWaitNs;)
+                    arrived = mbar_try_wait_parity(bar_s, 0u);
+                return;
+            }
+        } else {
+            cp_async_wait_all();
+        }
         __syncthreads();
         const unsigned char* ra = sa + (size_t)w0 * N * eb;
         const unsigned char* rb = gb ? sb + (size_t)w0 * N * eb : nullptr;

@@ -150,8 +150,10 @@ template <typename T, int N> struct L3 {
     // (16-byte aligned inputs of 4- or 8-byte values, tile fits shared memory)
     // nrows (0: all N^2): rows processed, from the row the pointers start at
     // (a multiple of the row tile RG::WZ)
+    // status (non-NULL): stage by bulk copies (cp.async.bulk, one per input
+    // array and tile) whose bounded wait sets *status to 1 if it expires
     static int fwd_z(cudaStream_t st, int kind, const void* a, const void* b, V* dst, int ds, int hout,
-                     const Tables<T>& tb, int stage = -1, size_t nrows = 0)
+                     const Tables<T>& tb, int stage = -1, size_t nrows = 0, int* status = nullptr, int tx_extra = 0)
     {
         const bool two = kind == SRC_XHI_F32 || kind == SRC_XHI_F64;
         const size_t eb = (kind == SRC_F32 || kind == SRC_XHI_F32) ? 4 : 8;
@@ -160,6 +162,12 @@ template <typename T, int N> struct L3 {
         const bool can_stage = kind != SRC_T && addr % 16 == 0 && smem_staged <= 227 * 1024;
         const unsigned blocks = (unsigned)((nrows ? nrows : (size_t)N * N) / RG::WZ);
         if (blocks == 0) return PS_OK;
+        if (stage != 0 && can_stage && status) {
+            PS_LTRY(set_smem(k_fwd_z<T, N, true, true>, smem_staged));
+            k_fwd_z<T, N, true, true><<<blocks, RG::THREADS, smem_staged, st>>>(kind, a, b, dst, ds, hout, 1, tb.twr,
+                                                                                 tb.twpp, status, tx_extra);
+            return PS_OK;
+        }
         if (stage != 0 && can_stage) {
             PS_LTRY(set_smem(k_fwd_z<T, N, true>, smem_staged));
             k_fwd_z<T, N, true><<<blocks, RG::THREADS, smem_staged, st>>>(kind, a, b, dst, ds, hout, 1, tb.twr,

@@ -115,7 +115,7 @@ def test_fault_spec_parsing(ps):
     """ps_gpu_debug_fault arms the host-side injector without touching a GPU;
     malformed specs are refused."""
     lib = ps.lib()
-    for good in (b"alloc:1", b"read:3", b"launch:2", b"alloc:5,read:1", b""):
+    for good in (b"alloc:1", b"read:3", b"launch:2", b"wait:1", b"alloc:5,read:1", b""):
         assert lib.ps_gpu_debug_fault(good) == 0, good
     for bad in (b"alloc", b"alloc:0", b"alloc:-2", b"disk:1", b"alloc:x", b"alloc:1,", b"launch:1x"):
         assert lib.ps_gpu_debug_fault(bad) == -1, bad

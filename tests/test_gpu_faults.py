@@ -97,3 +97,30 @@ def test_injected_failures_return_status_and_leak_nothing(gpu_lib, kind):
         assert hits >= 1
         # the device still works after all of that
         assert _scenario(ps, paths) == 0
+
+
+def test_bounded_wait_times_out_and_context_recovers(gpu_lib):
+    """The r2c pass of the field waits on an mbarrier for the bulk copies of
+    its input tile, for at most 0.2 s.  With "wait:1" armed, the barrier
+    expects 16 bytes more than the copies bring (they still complete), so the
+    wait runs out: the load returns PS_ERR_TIMEOUT, and the next load on the
+    same context gives the results of a normal one."""
+    import torch
+
+    ps = gpu_lib
+    dens = torch.from_numpy(synth.lognormal_density(N, 2.0, 7)).cuda()
+    cfgs, _, _ = ps.read_params_to_kvectors(N, BOX, 3, k1=0.15, k2=0.22, num_values=4, kbinningCase=ps.PS_BIN_DEFAULT)
+    with ps.Context(N, BOX, methods=ps.PS_FP32_BATCHED) as ctx:
+        ctx.get_FT_field(ps.PS_FIELD_DENS, dens)
+        B0, N0, _, _ = ctx.batch(cfgs, ps.PS_FP32_BATCHED)
+        ps.debug_fault("wait:1")
+        try:
+            with pytest.raises(ps.PsError) as err:
+                ctx.get_FT_field(ps.PS_FIELD_DENS, dens)
+            assert err.value.status == -5, err.value
+        finally:
+            ps.debug_fault(None)
+        ctx.get_FT_field(ps.PS_FIELD_DENS, dens)
+        B1, N1, _, _ = ctx.batch(cfgs, ps.PS_FP32_BATCHED)
+    np.testing.assert_array_equal(B1, B0)
+    np.testing.assert_array_equal(N1, N0)
