@@ -23,6 +23,7 @@
 
 #include "../../include/ps_gpu.h"
 #include "ps_launch.cuh"
+#include "ps_counts.cuh"
 
 namespace ps {
 PS_EXTERN_L3(float)
@@ -1370,89 +1371,6 @@ __global__ void k_round_counts(int n, const int* __restrict__ idx, double* __res
     if (q < n) sumI[idx[q]] = rint(sumI[idx[q]] / n3);
 }
 
-// ------------------------------------------------------------------ exact pair counts
-// Polygon counts of a pair group whose shells are all r^2 intervals, by
-// enumeration in integers instead of FP64 transforms of unit shells:
-//     count(c) = #{(m_a, m_b) in S_a x S_b : |w(m_a + m_b)|^2 in [r2lo_c, r2hi_c]},
-// w = componentwise wrap into the grid's lattice frequencies [-N/2, N/2)
-// (WRAP: only when a component can reach N/2; aliased triples are counted, as
-// the reference's N-grid sums count them).  That is the number of triples
-// m_a + m_b + m_c = 0 (mod N) with m_c in S_c (S_c = -S_c).  S_a enters as
-// representatives of its orbits under the 48 axis permutations and sign
-// flips with their orbit sizes as weights: S_b, the closing shells and |w(.)|^2
-// are invariant under them.  Each thread holds BPT modes of S_b and runs over
-// all representatives (staged in shared memory, read by every thread alike);
-// the CTA histograms |w(m_a + m_b)|^2 - s_lo over nbins bins in shared memory
-// (integer atomics: the result does not depend on their order), then sums
-// each closing shell's interval and adds it to counts[c].
-constexpr int kCountBPT = 2;
-constexpr int kCountRepChunk = 512;
-
-template <bool WRAP>
-__global__ void __launch_bounds__(256)
-    k_pair_counts(const int4* __restrict__ reps, int nrep, const short4* __restrict__ modes, int nb, int n, int s_lo,
-                  int nbins, const Shell* __restrict__ closing, int ncl, unsigned long long* __restrict__ counts)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    int4* srep = reinterpret_cast<int4*>(smem_raw);
-    unsigned int* hist = reinterpret_cast<unsigned int*>(smem_raw + kCountRepChunk * sizeof(int4));
-    for (int i = threadIdx.x; i < nbins; i += blockDim.x) hist[i] = 0u;
-    int bx[kCountBPT], by[kCountBPT], bz[kCountBPT];
-    bool bv[kCountBPT];
-#pragma unroll
-    for (int u = 0; u < kCountBPT; u++) {
-        const int idx = (blockIdx.x * kCountBPT + u) * blockDim.x + threadIdx.x;
-        bv[u] = idx < nb;
-        const short4 m = bv[u] ? modes[idx] : short4{0, 0, 0, 0};
-        bx[u] = m.x;
-        by[u] = m.y;
-        bz[u] = m.z;
-    }
-    const int half = n >> 1;
-    // representatives of this CTA's y-slice
-    const int per = (nrep + gridDim.y - 1) / gridDim.y;
-    const int r_begin = blockIdx.y * per, r_end = min(nrep, r_begin + per);
-    for (int r0 = r_begin; r0 < r_end; r0 += kCountRepChunk) {
-        const int cnt = min(kCountRepChunk, r_end - r0);
-        __syncthreads();
-        for (int i = threadIdx.x; i < cnt; i += blockDim.x) srep[i] = reps[r0 + i];
-        __syncthreads();
-        for (int r = 0; r < cnt; r++) {
-            const int4 a = srep[r];
-#pragma unroll
-            for (int u = 0; u < kCountBPT; u++) {
-                int qx = a.x + bx[u], qy = a.y + by[u], qz = a.z + bz[u];
-                if constexpr (WRAP) {
-                    qx += (qx < -half) * n - (qx >= half) * n;
-                    qy += (qy < -half) * n - (qy >= half) * n;
-                    qz += (qz < -half) * n - (qz >= half) * n;
-                }
-                const int sb = qx * qx + qy * qy + qz * qz - s_lo;
-                if (bv[u] && (unsigned)sb < (unsigned)nbins) atomicAdd(&hist[sb], (unsigned)a.w);
-            }
-        }
-    }
-    __syncthreads();
-    // closing shell c: the bins of its interval (clamped to the histogram)
-    const int lane = threadIdx.x & 31;
-    for (int c = 0; c < ncl; c++) {
-        const Shell sh = closing[c];
-        const int lo = max(sh.r2lo - s_lo, 0), hi = min(sh.r2hi - s_lo, nbins - 1);
-        unsigned long long v = 0ull;
-        for (int i = lo + (int)threadIdx.x; i <= hi; i += blockDim.x) v += hist[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0 && v) atomicAdd(&counts[c], v);
-    }
-}
-
-// sumI[idx[c]] = counts[c] (exact integers, below 2^53)
-__global__ void k_counts_out(int n, const unsigned long long* __restrict__ counts, const int* __restrict__ idx,
-                             double* __restrict__ sumI)
-{
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n) sumI[idx[c]] = (double)counts[c];
-}
 
 }  // namespace
 
@@ -1512,7 +1430,7 @@ struct LegKey {
 // the cyclic sums over the M-grid and over the N-grid count the same triples
 // (the reference's N-grid sums then have no aliased triples either); 2 b < M
 // keeps every mode of a shell on its own M-grid index.  N when none fits.
-const int kGridSizes[] = {16, 32, 64, 128, 192, 256, 320, 384, 512, 1024};
+const int kGridSizes[] = {16, 32, 64, 96, 128, 192, 256, 320, 384, 512, 1024};
 
 int alias_free_grid(int N, int ba, int bb, int bc)
 {
@@ -1641,89 +1559,6 @@ int scatter_dev(ps_gpu_ctx* c, const double* src, const int* didx, int count, do
 
 // Plan of the batched method: everything host-side happens here; the ops only
 // enqueue stream work (so a plan can be captured into a CUDA graph).
-// Mode lists of an exact pair count (k_pair_counts): the modes of S_b, the
-// orbit representatives of S_a with their orbit sizes, the histogram range.
-struct PairCountLists {
-    std::vector<short4> modes;
-    std::vector<int4> reps;
-    int s_lo = 0, nbins = 0;
-    bool wrap = false;
-};
-
-// Modes of an interval shell on the N-grid (lattice frequencies [-N/2, N/2)):
-// per (x, y) column the z with r2lo <= x^2 + y^2 + z^2 <= r2hi.
-std::vector<short4> interval_modes(const Shell& sh, int N)
-{
-    std::vector<short4> out;
-    const int b = std::min(sh.band, N / 2);
-    const int top = std::min(b, N / 2 - 1);
-    if (sh.r2hi < 0 || sh.r2lo > sh.r2hi) return out;
-    for (int x = -b; x <= top; x++)
-        for (int y = -b; y <= top; y++) {
-            const long long rest_hi = (long long)sh.r2hi - x * x - y * y;
-            if (rest_hi < 0) continue;
-            const long long rest_lo = (long long)sh.r2lo - x * x - y * y;
-            int zmax = (int)sqrt((double)rest_hi);
-            while ((long long)zmax * zmax > rest_hi) zmax--;
-            while ((long long)(zmax + 1) * (zmax + 1) <= rest_hi) zmax++;
-            int zmin = 0;
-            if (rest_lo > 0) {
-                zmin = (int)sqrt((double)rest_lo);
-                while ((long long)zmin * zmin < rest_lo) zmin++;
-                while (zmin > 0 && (long long)(zmin - 1) * (zmin - 1) >= rest_lo) zmin--;
-            }
-            for (int az = zmin; az <= zmax; az++) {
-                if (az <= top) out.push_back(short4{(short)x, (short)y, (short)az, 0});
-                if (az > 0 && az <= b) out.push_back(short4{(short)x, (short)y, (short)-az, 0});
-            }
-        }
-    return out;
-}
-
-// Canonical member of a mode's orbit under axis permutations and sign flips
-// on the N-grid: components |x| (as indices, -N/2 stays N/2 = -N/2), sorted.
-std::array<int, 3> orbit_key(int x, int y, int z)
-{
-    std::array<int, 3> k = {std::abs(x), std::abs(y), std::abs(z)};
-    std::sort(k.begin(), k.end());
-    return k;
-}
-
-// The lists of a group with interval legs a, b on an N-grid; false when the
-// enumeration does not apply (histogram too large for shared memory).
-bool pair_count_lists(const Shell& sa, const Shell& sb, int N, PairCountLists* L)
-{
-    constexpr int kMaxBins = 44 * 1024;  // 176 KB of uint32 bins beside the staged representatives
-    // host work O(b^2 + |S|); the enumeration itself |S_a| |S_b| / 48 pairs
-    const double est = 4.0 * 3.14159 * (double)std::max(sa.r2hi, 1) * 4.0 * 3.14159 * (double)std::max(sb.r2hi, 1);
-    if (std::max(sa.band, sb.band) > 300 || est / 48.0 > 4e10) return false;
-    std::vector<short4> ma = interval_modes(sa, N), mb = interval_modes(sb, N);
-    if ((double)ma.size() * (double)mb.size() / 48.0 > 4e9) return false;
-    if (ma.size() > mb.size()) std::swap(ma, mb);  // representatives from the smaller shell
-    std::map<std::array<int, 3>, int> orbits;
-    for (const short4& m : ma) orbits[orbit_key(m.x, m.y, m.z)]++;
-    L->reps.clear();
-    for (const auto& kv : orbits) {
-        // a representative as lattice frequencies (N/2 is the index of -N/2)
-        int v[3];
-        for (int q = 0; q < 3; q++) v[q] = kv.first[q] == N / 2 ? -(N / 2) : kv.first[q];
-        L->reps.push_back(int4{v[0], v[1], v[2], kv.second});
-    }
-    L->modes = mb;
-    const int bmax_a = std::min(sa.band, N / 2), bmax_b = std::min(sb.band, N / 2);
-    L->wrap = bmax_a + bmax_b >= N / 2;
-    const double ra_hi = sqrt((double)std::max(sa.r2hi, 0)), rb_hi = sqrt((double)std::max(sb.r2hi, 0));
-    const double ra_lo = sqrt((double)std::max(sa.r2lo, 0)), rb_lo = sqrt((double)std::max(sb.r2lo, 0));
-    double smax = (ra_hi + rb_hi) * (ra_hi + rb_hi);
-    if (L->wrap) smax = std::min(smax, 3.0 * (N / 2) * (N / 2));
-    const double dmin = L->wrap ? 0.0 : std::max({0.0, ra_lo - rb_hi, rb_lo - ra_hi});
-    L->s_lo = std::max(0, (int)floor(dmin * dmin) - 1);
-    const long long s_hi = (long long)ceil(smax) + 1;
-    if (s_hi - L->s_lo + 1 > kMaxBins || ma.empty() || mb.empty()) return false;
-    L->nbins = (int)(s_hi - L->s_lo + 1);
-    return true;
-}
-
 int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
 {
     if (!(c->methods & PS_FP32_BATCHED)) return fail(PS_ERR_ARG, "batched method not enabled for this context");
@@ -2076,21 +1911,34 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         const bool wrap = lists.wrap;
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        // one CTA per SM over about eight work items each: the count lane runs
+        // beside the two field lanes, and one histogram per SM leaves the rest
+        // of each SM's shared memory to their passes (a full wave of two CTAs
+        // per SM made the whole 64-configuration 512^3 step 6% slower)
+        const size_t csmem = kCountStageBytes + (size_t)nbins * sizeof(unsigned int);
+        int cgrid = 1, rep_slice = kCountRepChunk;
+        if (enum_counts) {
+            // the shared-memory limit is a property of the kernel, not of a
+            // launch (every group's launch, replayed from a graph too, must fit
+            // under it): the largest histogram any group may have
+            constexpr int kLimit = (int)(kCountStageBytes + kCountMaxBins * sizeof(unsigned int));
+            PS_CK(cudaFuncSetAttribute(k_pair_counts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLimit));
+            PS_CK(cudaFuncSetAttribute(k_pair_counts<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLimit));
+            const int nmc = (nmodes + 256 * kCountBPT - 1) / (256 * kCountBPT);
+            const int nrs = std::min(nrep, std::max(1, (8 * sms + nmc - 1) / nmc));
+            rep_slice = std::min(kCountRepChunk, std::max(8, (nrep + nrs - 1) / nrs));
+            const int nitems = nmc * ((nrep + rep_slice - 1) / rep_slice);
+            cgrid = std::max(1, std::min(nitems, sms));
+        }
         auto enum_part = [=]() -> int {
             PS_CK(cudaMemsetAsync(dcounts, 0, sizeof(unsigned long long) * ng, c->stream));
-            const int bx = (nmodes + 256 * kCountBPT - 1) / (256 * kCountBPT);
-            const int by = std::max(1, std::min((2 * sms + bx - 1) / bx, (nrep + 63) / 64));
-            const size_t smem = kCountRepChunk * sizeof(int4) + (size_t)nbins * sizeof(unsigned int);
             Prof pf(c);
-            if (wrap) {
-                PS_CK(cudaFuncSetAttribute(k_pair_counts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                k_pair_counts<true><<<dim3(bx, by), 256, smem, c->stream>>>(dreps, nrep, dmodes, nmodes, N, s_lo, nbins,
-                                                                            dtable + go, ng, dcounts);
-            } else {
-                PS_CK(cudaFuncSetAttribute(k_pair_counts<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                k_pair_counts<false><<<dim3(bx, by), 256, smem, c->stream>>>(dreps, nrep, dmodes, nmodes, N, s_lo,
-                                                                             nbins, dtable + go, ng, dcounts);
-            }
+            if (wrap)
+                k_pair_counts<true><<<cgrid, 256, csmem, c->stream>>>(dreps, nrep, dmodes, nmodes, N, s_lo, nbins,
+                                                                      rep_slice, dtable + go, ng, dcounts);
+            else
+                k_pair_counts<false><<<cgrid, 256, csmem, c->stream>>>(dreps, nrep, dmodes, nmodes, N, s_lo, nbins,
+                                                                       rep_slice, dtable + go, ng, dcounts);
             pf.end(KF_PAIR_COUNTS, 8.0 * nmodes + 16.0 * nrep);
             k_counts_out<<<(ng + 127) / 128, 128, 0, c->stream>>>(ng, dcounts, didx + io, sumI);
             PS_CK(launch_status());

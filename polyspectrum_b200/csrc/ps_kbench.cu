@@ -17,6 +17,7 @@
 #include <cmath>
 #include <algorithm>
 #include "ps_launch.cuh"
+#include "ps_counts.cuh"
 
 namespace ps {
 int launch_fail(cudaError_t e, const char* what)
@@ -24,6 +25,9 @@ int launch_fail(cudaError_t e, const char* what)
     fprintf(stderr, "%s: %s\n", what, cudaGetErrorString(e));
     return 1;
 }
+template struct L3<float, 96>;
+template struct L3<float, 128>;
+template struct L3<float, 300>;
 template struct L3<float, 320>;
 template struct L3<float, 384>;
 template struct L3<float, 512>;
@@ -149,6 +153,47 @@ double time_pair(int reps, const float2* wa, int Sa, int ba, const float2* wb, i
     CK(cudaFree((void*)twr));
     return ms / reps;
 }
+
+// Mean time of `reps` launches of the exact-count kernel <WRAP, BPT> on the
+// lists L (closing shells dcl, ncl of them) with `grid` CTAs over work items
+// of rep_slice representatives; the counts of the last launch go to hc.
+template <bool WRAP, int BPT>
+double time_counts(int reps, const PairCountLists& L, const int4* dreps, const short4* dmodes, int N,
+                   const Shell* dcl, int ncl, unsigned long long* dcounts, int rep_slice, bool one_wave,
+                   std::vector<unsigned long long>& hc)
+{
+    const int nrep = (int)L.reps.size(), nb = (int)L.modes.size();
+    rep_slice = std::max(1, std::min(rep_slice, kCountRepChunk));
+    const size_t smem = kCountStageBytes + (size_t)L.nbins * sizeof(unsigned int);
+    auto kern = k_pair_counts<WRAP, BPT>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    const int nmc = (nb + 256 * BPT - 1) / (256 * BPT), nitems = nmc * ((nrep + rep_slice - 1) / rep_slice);
+    const int grid = one_wave ? std::min(nitems, std::max(per_sm, 1) * sms) : nitems;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float total = 0.f;
+    for (int it = 0; it < reps + 2; it++) {
+        CK(cudaMemset(dcounts, 0, sizeof(unsigned long long) * ncl));
+        CK(cudaEventRecord(e0));
+        kern<<<grid, 256, smem>>>(dreps, nrep, dmodes, nb, N, L.s_lo, L.nbins, rep_slice, dcl, ncl, dcounts);
+        CK(cudaEventRecord(e1));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (it >= 2) total += ms;
+    }
+    CK(cudaGetLastError());
+    hc.assign(ncl, 0ull);
+    CK(cudaMemcpy(hc.data(), dcounts, sizeof(unsigned long long) * ncl, cudaMemcpyDeviceToHost));
+    printf("pair_counts wrap=%d BPT=%d slice=%d %s: %.4f ms  (%d CTAs, %d CTAs/SM, %zu B smem)\n", (int)WRAP, BPT,
+           rep_slice, one_wave ? "one wave" : "one item per CTA", total / reps, grid, per_sm, smem);
+    return total / reps;
+}
 struct Timer {
     std::vector<cudaEvent_t> ev; std::vector<double> acc; int k = 0;
     Timer(int n) : ev(n + 1), acc(n, 0.0) { for (auto& e : ev) CK(cudaEventCreate(&e)); }
@@ -242,6 +287,69 @@ int main(int argc, char** argv)
         time_pair<320, 0, false>(reps, wa, Sa2, a2, wb, Sb2, b2, w3, S2, c2, T2.twpp);
         time_pair<320, 0, true>(reps, wa, Sa2, a2, wb, Sb2, b2, w3, S2, c2, T2.twpp);
         time_pair<320, 20, true>(reps, wa, Sa2, a2, wb, Sb2, b2, w3, S2, c2, T2.twpp);
+        // the same group on a 300-point sub-grid (also alias-free: 52 + 77 + 128 < 300)
+        Tables<float> T300 = make_tables<300>();
+        time_pair<300, 0, false>(reps, wa, Sa2, a2, wb, Sb2, b2, w3, S2, c2, T300.twpp);
+        time_pass_y<320, true, 0>(reps, wb, Sb2, Sb2, b2, 320, "inv B");
+        time_pass_y<300, true, 0>(reps, wb, Sb2, Sb2, b2, 300, "inv B");
+        time_pass_y<320, false, 0>(reps, w3, S2, S2, 320, c2, "fwd");
+        time_pass_y<300, false, 0>(reps, w3, S2, S2, 300, c2, "fwd");
+    }
+    {
+        // the smallest group of the sweep (leg bands 13 and 32, closing band 45)
+        // on its 128-point grid and on a 96-point grid (13 + 32 + 45 < 96)
+        const int a1 = 13, b1 = 32, c1 = 45;
+        const int Sa1 = rup(a1 + 1, 16), Sb1 = rup(b1 + 1, 16), S1 = rup(c1 + 1, 16);
+        Tables<float> T128 = make_tables<128>(), T96 = make_tables<96>();
+        time_pair<128, 0, false>(reps, wa, Sa1, a1, wb, Sb1, b1, w3, S1, c1, T128.twpp);
+        time_pair<96, 0, false>(reps, wa, Sa1, a1, wb, Sb1, b1, w3, S1, c1, T96.twpp);
+        time_pass_y<128, true, 0>(reps, wb, Sb1, Sb1, b1, 128, "inv B");
+        time_pass_y<96, true, 0>(reps, wb, Sb1, Sb1, b1, 96, "inv B");
+        time_pass_y<128, false, 0>(reps, w3, S1, S1, 128, c1, "fwd");
+        time_pass_y<96, false, 0>(reps, w3, S1, S1, 96, c1, "fwd");
+    }
+    {
+        // exact polygon counts of the largest group: legs |m| in [63.5, 64.5]
+        // and [95.5, 96.5], 16 closing shells covering |m| in [32, 161]
+        const int NG = 512;
+        auto shell = [](double lo, double hi) {
+            Shell sh{};
+            sh.kind = SHELL_DEFAULT;
+            sh.r2lo = (int)std::ceil(lo * lo);
+            sh.r2hi = (int)std::floor(hi * hi);
+            sh.band = (int)std::ceil(hi);
+            return sh;
+        };
+        const Shell sa = shell(63.5, 64.5), sb = shell(95.5, 96.5);
+        std::vector<Shell> cl;
+        for (int q = 0; q < 16; q++) cl.push_back(shell(32.0 + 8.0 * q, 32.0 + 8.0 * q + 16.0));
+        PairCountLists L;
+        if (!pair_count_lists(sa, sb, NG, &L)) { fprintf(stderr, "count lists refused\n"); return 1; }
+        int4* dreps; short4* dmodes; Shell* dcl; unsigned long long* dcnt;
+        CK(cudaMalloc(&dreps, L.reps.size() * sizeof(int4)));
+        CK(cudaMalloc(&dmodes, L.modes.size() * sizeof(short4)));
+        CK(cudaMalloc(&dcl, cl.size() * sizeof(Shell)));
+        CK(cudaMalloc(&dcnt, cl.size() * sizeof(unsigned long long)));
+        CK(cudaMemcpy(dreps, L.reps.data(), L.reps.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dmodes, L.modes.data(), L.modes.size() * sizeof(short4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dcl, cl.data(), cl.size() * sizeof(Shell), cudaMemcpyHostToDevice));
+        printf("pair_counts lists: %zu representatives, %zu modes, %d bins, wrap %d\n", L.reps.size(), L.modes.size(),
+               L.nbins, (int)L.wrap);
+        const int nrep = (int)L.reps.size();
+        std::vector<unsigned long long> ref, got;
+        time_counts<true, 2>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, (nrep + 1) / 2, false, ref);
+        auto check = [&](const std::vector<unsigned long long>& v) {
+            if (v != ref) { fprintf(stderr, "pair_counts variant disagrees\n"); exit(1); }
+        };
+        time_counts<false, 2>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, (nrep + 1) / 2, false, got); check(got);
+        time_counts<false, 4>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, (nrep + 2) / 3, false, got); check(got);
+        for (int slice : {16, 32, 64, 128}) {
+            time_counts<false, 2>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, slice, true, got); check(got);
+            time_counts<false, 4>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, slice, true, got); check(got);
+            time_counts<true, 2>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, slice, true, got); check(got);
+        }
+        time_counts<false, 1>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, 64, true, got); check(got);
+        time_counts<false, 8>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, 64, true, got); check(got);
     }
     return 0;
 }
