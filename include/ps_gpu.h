@@ -234,6 +234,18 @@ int ps_gpu_synchronize(ps_gpu_ctx *ctx);
  * execution, as ps_gpu_plan_execute does.  For loops whose per-field results
  * are not needed on the host every time.  No reference counterpart. */
 int ps_gpu_plan_launch(ps_gpu_ctx *ctx, ps_gpu_plan *plan);
+/* Queues the parts of a PS_FP32_BATCHED plan's next execution that read no
+ * field (the DERIVED k-ranges, the closing shells' tables and the exact
+ * polygon counts) on the context's side stream, after the work already on
+ * its stream.  The plan's next ps_gpu_plan_execute / _submit / _launch then
+ * runs only the field parts on the stream, waiting for the prepared parts
+ * where it reads them.  A field load queued between the two
+ * (ps_gpu_set_field / _async) overlaps the prepared parts.  Every execution
+ * still computes all of its results; a prepared execution's results are
+ * identical to an unprepared one's.  No-op while per-kernel profiling is on,
+ * or when already prepared.  No reference counterpart (run.c:98-120 loads
+ * the field, then evaluates the configurations one after another). */
+int ps_gpu_plan_prepare(ps_gpu_ctx *ctx, ps_gpu_plan *plan);
 int ps_gpu_plan_results(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *Npoly,
                         double *kappa_or_NULL, ps_cfg *cfgs_out_or_NULL);
 /* Queues, on the context's stream, a copy of the latest execution's results

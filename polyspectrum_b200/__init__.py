@@ -104,6 +104,7 @@ def lib() -> C.CDLL:
     L.ps_gpu_keep_modulus.argtypes = [vp, ip]
     L.ps_gpu_set_spectrum_band.argtypes = [vp, ip]
     L.ps_gpu_plan_launch.argtypes = [vp, vp]
+    L.ps_gpu_plan_prepare.argtypes = [vp, vp]
     L.ps_gpu_plan_results.argtypes = [vp, vp, dp, dp, dp, C.POINTER(ps_cfg)]
     L.ps_gpu_plan_band.argtypes = [vp]
     L.ps_gpu_tune_import.argtypes = [vp, C.c_char_p]
@@ -121,7 +122,8 @@ def lib() -> C.CDLL:
                  "ps_gpu_kernel_stats", "ps_gpu_plan_create", "ps_gpu_plan_execute",
                  "ps_gpu_set_field_async", "ps_gpu_plan_submit", "ps_gpu_synchronize",
                  "ps_gpu_tune_export", "ps_gpu_tune_import", "ps_gpu_keep_modulus",
-                 "ps_gpu_set_spectrum_band", "ps_gpu_plan_band", "ps_gpu_plan_launch", "ps_gpu_plan_results",
+                 "ps_gpu_set_spectrum_band", "ps_gpu_plan_band", "ps_gpu_plan_launch", "ps_gpu_plan_prepare",
+                 "ps_gpu_plan_results",
                  "ps_gpu_set_field_files", "ps_gpu_load_stats", "ps_gpu_debug_fault",
                  "ps_gpu_plan_results_device"):
         getattr(L, name).restype = ip
@@ -400,6 +402,12 @@ class Plan:
     def launch(self):
         """Queue one execution, results left on the device (ps_gpu_plan_launch)."""
         _check(lib().ps_gpu_plan_launch(self.ctx.handle, self._h))
+
+    def prepare(self):
+        """Queue the field-independent parts of the next execution (DERIVED
+        k-ranges, exact counts) on the side stream, so that a field load queued
+        next overlaps them (ps_gpu_plan_prepare)."""
+        _check(lib().ps_gpu_plan_prepare(self.ctx.handle, self._h))
 
     def results(self):
         """Results of the latest execution (waits): (B, Npoly, kappa, cfgs_out)."""

@@ -1379,7 +1379,13 @@ struct ps_gpu_plan {
     ps_gpu_ctx* ctx = nullptr;
     int method = 0, nconf = 0, flags = 0;
     std::vector<ps_cfg> cfgs;
-    std::vector<std::function<int()>> ops;  // the launch sequence (stream work only)
+    // the launch sequence (stream work only; every op enqueues on the
+    // context's current stream), split by what each part reads:
+    std::vector<std::function<int()>> ops;         // DERIVED k-ranges and closing shells
+    std::vector<std::function<int()>> ops_counts;  // exact polygon counts per pair group (no field)
+    std::vector<std::function<int()>> ops_groups;  // the pair groups' field parts (main or second lane)
+    std::vector<std::function<int()>> ops_tail;    // n = 2 and leg-by-leg configurations, finalisation
+    bool has_groups = false;
     std::vector<void*> owned;               // device buffers of this plan
     double* dres = nullptr;                 // B, Npoly per configuration
     double* dsumA = nullptr;                // sum |terms| (condition numbers)
@@ -1392,6 +1398,16 @@ struct ps_gpu_plan {
     cudaGraphExec_t exec = nullptr;
     long long graph_launches = 0;  // kernels in the captured graph
     int band = 0;                  // largest |component| of a mode the plan reads
+    // ps_gpu_plan_prepare: the field-independent parts (ops, ops_counts) of
+    // the next execution enqueued ahead on the side lane; ev_derived and
+    // ev_counts mark their ends there
+    bool prepared = false;
+    cudaEvent_t ev_prep = nullptr, ev_derived = nullptr, ev_counts = nullptr;
+    struct Part {  // one part captured as a graph (PS_PLAN_GRAPH)
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;
+    } parts[4];  // derived, counts, groups, tail
 };
 
 namespace {
@@ -2023,42 +2039,25 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             PS_TRY(ensure_lut(c, (size_t)3 * (N / 2) * (N / 2) + 2));
         }
     }
-    if (!groups.empty()) {  // fork the side and second lanes (after the DERIVED chain the groups read)
-        ops.push_back([=]() {
-            PS_CK(cudaEventRecord(c->ev_fork, c->stream));
-            PS_CK(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
-            if (!c->prof_on) PS_CK(cudaStreamWaitEvent(c->lane2_stream, c->ev_fork, 0));
-            return PS_OK;
-        });
-    }
+    // the groups' counts (run on the side lane) and field parts (main or
+    // second lane); the lanes are forked and joined where the parts are enqueued
+    P->has_groups = !groups.empty();
     for (size_t g = 0; g < groups.size(); g++) {
-        const auto dop = group_dop[g], iop = group_iop[g];
+        const auto dop = group_dop[g];
         const bool second = group_lane[g] == 1;
-        ops.push_back([=]() {
+        P->ops_counts.push_back(group_iop[g]);
+        P->ops_groups.push_back([=]() {
             if (second) {
                 Lane2 lane(c);
-                PS_TRY(dop());
-            } else {
-                PS_TRY(dop());
+                return dop();
             }
-            SideLane lane(c);
-            return iop();
+            return dop();
         });
     }
-    if (!groups.empty()) {  // join the side and second lanes
-        ops.push_back([=]() {
-            PS_CK(cudaEventRecord(c->ev_join, c->side_stream));
-            PS_CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
-            if (!c->prof_on) {
-                PS_CK(cudaEventRecord(c->ev_join2, c->lane2_stream));
-                PS_CK(cudaStreamWaitEvent(c->stream, c->ev_join2, 0));
-            }
-            return PS_OK;
-        });
-    }
+    auto& tail = P->ops_tail;
     // ---- n = 2 (Parseval): one k-space pass per chunk
     for (const P2Chunk ch : p2) {
-        ops.push_back([=]() {
+        tail.push_back([=]() {
             const unsigned short* lut = nullptr;
             if (ch.lut_ok) {
                 Prof pf(c);
@@ -2094,7 +2093,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         }
         std::vector<int> bands;
         for (auto& pr : up) bands.push_back(host_shell_of(pr.first).band);
-        ops.push_back([=]() {
+        tail.push_back([=]() {
             const int r = (int)up.size();
             for (int pass = 0; pass < 2; pass++)
                 for (int x = 0; x < r; x++) {
@@ -2116,7 +2115,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
     }
     if (!direct.empty()) {
         const int nr = (int)direct.size();
-        ops.push_back([=]() {
+        tail.push_back([=]() {
             Prof pf(c);
             k_round_counts<<<(nr + 127) / 128, 128, 0, c->stream>>>(nr, dround, sumI, n3);
             pf.end(KF_FINAL, 0.0);
@@ -2124,7 +2123,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         });
     }
     double* dres = P->dres;
-    ops.push_back([=]() {
+    tail.push_back([=]() {
         Prof pf(c);
         k_finalize<<<(nconf + 127) / 128, 128, 0, c->stream>>>(nconf, dcoef, sumD, sumI, 1.0 / n3, 1, dres);
         pf.end(KF_FINAL, 0.0);
@@ -2134,10 +2133,60 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
     return PS_OK;
 }
 
+// The plan's parts (ps_gpu_plan::parts): 0 DERIVED chain, 1 counts, 2 the
+// groups' field parts with the second lane forked and joined, 3 the tail.
+enum PlanPart : int { PART_DERIVED = 0, PART_COUNTS = 1, PART_GROUPS = 2, PART_TAIL = 3 };
+
+int enqueue_ops(const std::vector<std::function<int()>>& ops)
+{
+    for (auto& op : ops) PS_TRY(op());
+    return PS_OK;
+}
+
+int enqueue_part(ps_gpu_ctx* c, ps_gpu_plan* P, int part)
+{
+    switch (part) {
+    case PART_DERIVED:
+        return enqueue_ops(P->ops);
+    case PART_COUNTS:
+        return enqueue_ops(P->ops_counts);
+    case PART_GROUPS:
+        if (P->has_groups && !c->prof_on) {
+            PS_CK(cudaEventRecord(c->ev_fork, c->stream));
+            PS_CK(cudaStreamWaitEvent(c->lane2_stream, c->ev_fork, 0));
+        }
+        PS_TRY(enqueue_ops(P->ops_groups));
+        if (P->has_groups && !c->prof_on) {
+            PS_CK(cudaEventRecord(c->ev_join2, c->lane2_stream));
+            PS_CK(cudaStreamWaitEvent(c->stream, c->ev_join2, 0));
+        }
+        return PS_OK;
+    default:
+        return enqueue_ops(P->ops_tail);
+    }
+}
+
+// The whole execution on the context's stream: the DERIVED chain, then the
+// counts on the side lane beside the groups' field parts, then the tail.
 int plan_enqueue(ps_gpu_ctx* c, ps_gpu_plan* P)
 {
-    for (auto& op : P->ops) PS_TRY(op());
-    return PS_OK;
+    if (P->prepared) {  // a prepared part may still write the plan's tables and counts
+        PS_CK(cudaStreamWaitEvent(c->stream, P->ev_counts, 0));
+        P->prepared = false;
+    }
+    PS_TRY(enqueue_part(c, P, PART_DERIVED));
+    if (P->has_groups) {  // fork the side lane after the DERIVED chain the counts read
+        PS_CK(cudaEventRecord(c->ev_fork, c->stream));
+        PS_CK(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
+        {
+            SideLane lane(c);
+            PS_TRY(enqueue_part(c, P, PART_COUNTS));
+        }
+        PS_TRY(enqueue_part(c, P, PART_GROUPS));
+        PS_CK(cudaEventRecord(c->ev_join, c->side_stream));
+        PS_CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    }
+    return enqueue_part(c, P, PART_TAIL);
 }
 
 // Results of an executed batched plan: device -> pinned host copy (stream
@@ -2247,6 +2296,19 @@ void plan_release(ps_gpu_plan* P)
     if (P->graph) cudaGraphDestroy(P->graph);
     P->exec = nullptr;
     P->graph = nullptr;
+    for (auto& q : P->parts) {
+        if (q.exec) cudaGraphExecDestroy(q.exec);
+        if (q.graph) cudaGraphDestroy(q.graph);
+        q = ps_gpu_plan::Part{};
+    }
+    for (cudaEvent_t* e : {&P->ev_prep, &P->ev_derived, &P->ev_counts}) {
+        if (*e) cudaEventDestroy(*e);
+        *e = nullptr;
+    }
+    P->prepared = false;
+    P->ops_counts.clear();
+    P->ops_groups.clear();
+    P->ops_tail.clear();
     for (void* p : P->owned) cudaFree(p);
     P->owned.clear();
     if (P->hres) cudaFreeHost(P->hres);
@@ -2261,10 +2323,12 @@ void plan_free(ps_gpu_plan* P)
     delete P;
 }
 
-int plan_run(ps_gpu_ctx* c, ps_gpu_plan* P)
+// Captures fn's stream work on the context's current stream into *g / *x
+// (first use), then launches it there; kernels counted once per launch.
+int capture_launch(ps_gpu_ctx* c, cudaGraph_t* g, cudaGraphExec_t* x, long long* nlaunch,
+                   const std::function<int()>& fn)
 {
-    if (!(P->flags & PS_PLAN_GRAPH)) return plan_enqueue(c, P);
-    if (!P->exec) {
+    if (!*x) {
         c->capturing = true;
         const long long before = c->launches;
         cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
@@ -2272,23 +2336,67 @@ int plan_run(ps_gpu_ctx* c, ps_gpu_plan* P)
             c->capturing = false;
             return fail(PS_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
         }
-        const int rc = plan_enqueue(c, P);
-        cudaGraph_t g = nullptr;
-        e = cudaStreamEndCapture(c->stream, &g);
+        const int rc = fn();
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(c->stream, &gr);
         c->capturing = false;
         if (rc != PS_OK) {
-            if (g) cudaGraphDestroy(g);
+            if (gr) cudaGraphDestroy(gr);
             return rc;
         }
         if (e != cudaSuccess) return fail(PS_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
-        P->graph = g;
-        P->graph_launches = c->launches - before;
+        *g = gr;
+        *nlaunch = c->launches - before;
         c->launches = before;
-        PS_CK(cudaGraphInstantiate(&P->exec, P->graph, 0));
+        PS_CK(cudaGraphInstantiate(x, gr, 0));
     }
-    PS_CK(cudaGraphLaunch(P->exec, c->stream));
-    c->launches += P->graph_launches;
-    c->launches_total += P->graph_launches;
+    PS_CK(cudaGraphLaunch(*x, c->stream));
+    c->launches += *nlaunch;
+    c->launches_total += *nlaunch;
+    return PS_OK;
+}
+
+// One part on the context's current stream: replayed from its graph
+// (PS_PLAN_GRAPH) or enqueued launch by launch.
+int run_part(ps_gpu_ctx* c, ps_gpu_plan* P, int part)
+{
+    if (!(P->flags & PS_PLAN_GRAPH)) return enqueue_part(c, P, part);
+    ps_gpu_plan::Part& q = P->parts[part];
+    return capture_launch(c, &q.graph, &q.exec, &q.launches, [=]() { return enqueue_part(c, P, part); });
+}
+
+// One execution of the plan on the context's stream.  After
+// ps_gpu_plan_prepare: the groups' field parts wait for the prepared DERIVED
+// chain, the tail for the prepared counts.  Else the whole sequence, replayed
+// from one graph (PS_PLAN_GRAPH) or enqueued launch by launch.
+int plan_run(ps_gpu_ctx* c, ps_gpu_plan* P)
+{
+    if (P->prepared) {
+        P->prepared = false;
+        PS_CK(cudaStreamWaitEvent(c->stream, P->ev_derived, 0));
+        PS_TRY(run_part(c, P, PART_GROUPS));
+        PS_CK(cudaStreamWaitEvent(c->stream, P->ev_counts, 0));
+        return run_part(c, P, PART_TAIL);
+    }
+    if (!(P->flags & PS_PLAN_GRAPH)) return plan_enqueue(c, P);
+    return capture_launch(c, &P->graph, &P->exec, &P->graph_launches, [=]() { return plan_enqueue(c, P); });
+}
+
+// Enqueues the field-independent parts of the plan's next execution (the
+// DERIVED chain and the exact counts) on the side lane, after the work
+// already on the context's stream.
+int plan_prepare(ps_gpu_ctx* c, ps_gpu_plan* P)
+{
+    for (cudaEvent_t* e : {&P->ev_prep, &P->ev_derived, &P->ev_counts})
+        if (!*e) PS_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    PS_CK(cudaEventRecord(P->ev_prep, c->stream));
+    PS_CK(cudaStreamWaitEvent(c->side_stream, P->ev_prep, 0));
+    SideLane lane(c, true);
+    PS_TRY(run_part(c, P, PART_DERIVED));
+    PS_CK(cudaEventRecord(P->ev_derived, c->stream));
+    PS_TRY(run_part(c, P, PART_COUNTS));
+    PS_CK(cudaEventRecord(P->ev_counts, c->stream));
+    P->prepared = true;
     return PS_OK;
 }
 
@@ -3147,7 +3255,8 @@ void ps_gpu_plan_destroy(ps_gpu_plan* P)
     if (!P) return;
     if (P->ctx) {
         cudaSetDevice(P->ctx->device);
-        cudaStreamSynchronize(P->ctx->stream);  // submissions still reading it
+        cudaStreamSynchronize(P->ctx->stream);       // submissions still reading it
+        cudaStreamSynchronize(P->ctx->side_stream);  // and a prepared part still writing it
         drain_pending(P->ctx, true);            // and those not yet unpacked
         P->ctx->plans.erase(P);
     }
@@ -3199,6 +3308,17 @@ int ps_gpu_plan_launch(ps_gpu_ctx* c, ps_gpu_plan* P)
     PS_CK(cudaSetDevice(c->device));
     if ((P->flags & PS_PLAN_GRAPH) && c->prof_on) return plan_enqueue(c, P);
     return plan_run(c, P);
+}
+
+int ps_gpu_plan_prepare(ps_gpu_ctx* c, ps_gpu_plan* P)
+{
+    g_err[0] = 0;
+    if (!c || !P) return fail(PS_ERR_ARG, "NULL argument");
+    if (P->ctx != c) return fail(PS_ERR_ARG, "plan belongs to another context");
+    if (P->method != PS_FP32_BATCHED) return fail(PS_ERR_UNSUPPORTED, "preparing needs a PS_FP32_BATCHED plan");
+    if (P->nconf == 0 || c->prof_on || P->prepared) return PS_OK;  // profiled executions stay on one lane
+    PS_CK(cudaSetDevice(c->device));
+    return plan_prepare(c, P);
 }
 
 int ps_gpu_plan_results(ps_gpu_ctx* c, ps_gpu_plan* P, double* B, double* Npoly, double* kappa, ps_cfg* cfgs_out)

@@ -212,6 +212,84 @@ def test_plan_replay_matches_batch(gpu_lib, graph):
         plan.close()
 
 
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+def test_prepared_plan_matches_batch(gpu_lib, graph):
+    """ps_gpu_plan_prepare queued before the field load (the DERIVED chain and
+    the exact counts on the side stream, overlapping the load) gives exactly
+    the eager batch's results on every field, through execute, submit and
+    launch; so do two plans prepared and executed in the opposite order, a
+    prepare repeated, a prepared plan executed with per-kernel profiling on
+    (eager on one lane) and a prepared plan counting with FP64 transforms."""
+    import torch
+    ps = gpu_lib
+    n_grid, box = 32, 200.0
+    d1, x1 = fields(n_grid, box)
+    d2, x2 = fields(n_grid, box, seed=7)
+    cfgs = []
+    for k1, k2 in ((0.1, 0.14), (0.12, 0.2)):
+        c, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1, k2=k2, num_values=5, kbinningCase=1)
+        cfgs += [c[i] for i in range(len(c))]
+    eq, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, equilateral=1, num_values=3)
+    p2, _, _ = ps.read_params_to_kvectors(n_grid, box, 2, num_values=2)
+    cfgs += [eq[i] for i in range(len(eq))] + [p2[i] for i in range(len(p2))]
+    other = cfgs[:5]
+    with ps.Context(n_grid, box) as ctx:
+        plan = ctx.plan(cfgs, graph=graph, kappa=True)
+        plan_b = ctx.plan(other, graph=graph)
+        plan_f = ctx.plan(cfgs, graph=graph, fft_counts=True)
+
+        def expect(dens, xhii, cf, kap=True):
+            dd, xx = field_args(2, dens, xhii)
+            ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+            return ctx.batch(cf, ps.PS_FP32_BATCHED, kappa=kap)
+
+        def same(got, ref, n):
+            np.testing.assert_array_equal(got[0], ref[0])
+            np.testing.assert_array_equal(got[1], ref[1])
+            if got[2] is not None and ref[2] is not None:
+                np.testing.assert_array_equal(got[2], ref[2])
+            for i in range(n):
+                assert list(got[3][i].kmin)[:3] == list(ref[3][i].kmin)[:3]
+                assert list(got[3][i].kmax)[:3] == list(ref[3][i].kmax)[:3]
+
+        for dens, xhii in ((d1, x1), (d2, x2), (d1, x1)):
+            ref = expect(dens, xhii, cfgs)
+            dd, xx = field_args(2, dens, xhii)
+            # execute
+            plan.prepare()
+            plan.prepare()  # already prepared: no-op
+            ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+            same(plan.execute(), ref, len(cfgs))
+            # launch, results read later
+            plan.prepare()
+            ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+            plan.launch()
+            same(plan.results(), ref, len(cfgs))
+            # two plans prepared, executed in the opposite order
+            ref_b = expect(dens, xhii, other, kap=False)
+            plan.prepare()
+            plan_b.prepare()
+            ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+            same(plan_b.execute(), ref_b, len(other))
+            same(plan.execute(), ref, len(cfgs))
+            # prepared, then executed with per-kernel profiling on
+            plan.prepare()
+            ctx.set_profiling(True)
+            try:
+                same(plan.execute(), ref, len(cfgs))
+            finally:
+                ctx.set_profiling(False)
+            # FP64 transform counts, prepared
+            plan_f.prepare()
+            ctx.get_FT_field(2, dd, xx, use_only_phase=1)
+            got = plan_f.execute()
+            same((got[0], got[1], None, got[3]), (ref[0], ref[1], None, ref[3]), len(cfgs))
+        torch.cuda.synchronize()
+        plan.close()
+        plan_b.close()
+        plan_f.close()
+
+
 @pytest.mark.parametrize("pinned", [False, True], ids=["pageable", "pinned"])
 def test_async_pipeline_matches_sync(gpu_lib, pinned):
     """Fields uploaded with set_field_async and plans submitted without waiting
