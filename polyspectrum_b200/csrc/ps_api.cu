@@ -1927,10 +1927,10 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
         const bool wrap = lists.wrap;
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-        // one CTA per SM over about eight work items each: the count lane runs
-        // beside the two field lanes, and one histogram per SM leaves the rest
-        // of each SM's shared memory to their passes (a full wave of two CTAs
-        // per SM made the whole 64-configuration 512^3 step 6% slower)
+        // one CTA of kCountThreads per SM over about eight work items each: the
+        // count lane runs beside the field load and the field lanes, and one
+        // histogram per SM leaves the rest of each SM's shared memory to their
+        // passes
         const size_t csmem = kCountStageBytes + (size_t)nbins * sizeof(unsigned int);
         int cgrid = 1, rep_slice = kCountRepChunk;
         if (enum_counts) {
@@ -1940,7 +1940,7 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             constexpr int kLimit = (int)(kCountStageBytes + kCountMaxBins * sizeof(unsigned int));
             PS_CK(cudaFuncSetAttribute(k_pair_counts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLimit));
             PS_CK(cudaFuncSetAttribute(k_pair_counts<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLimit));
-            const int nmc = (nmodes + 256 * kCountBPT - 1) / (256 * kCountBPT);
+            const int nmc = (nmodes + kCountThreads * kCountBPT - 1) / (kCountThreads * kCountBPT);
             const int nrs = std::min(nrep, std::max(1, (8 * sms + nmc - 1) / nmc));
             rep_slice = std::min(kCountRepChunk, std::max(8, (nrep + nrs - 1) / nrs));
             const int nitems = nmc * ((nrep + rep_slice - 1) / rep_slice);
@@ -1950,11 +1950,11 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             PS_CK(cudaMemsetAsync(dcounts, 0, sizeof(unsigned long long) * ng, c->stream));
             Prof pf(c);
             if (wrap)
-                k_pair_counts<true><<<cgrid, 256, csmem, c->stream>>>(dreps, nrep, dmodes, nmodes, N, s_lo, nbins,
-                                                                      rep_slice, dtable + go, ng, dcounts);
+                k_pair_counts<true><<<cgrid, kCountThreads, csmem, c->stream>>>(
+                    dreps, nrep, dmodes, nmodes, N, s_lo, nbins, rep_slice, dtable + go, ng, dcounts);
             else
-                k_pair_counts<false><<<cgrid, 256, csmem, c->stream>>>(dreps, nrep, dmodes, nmodes, N, s_lo, nbins,
-                                                                       rep_slice, dtable + go, ng, dcounts);
+                k_pair_counts<false><<<cgrid, kCountThreads, csmem, c->stream>>>(
+                    dreps, nrep, dmodes, nmodes, N, s_lo, nbins, rep_slice, dtable + go, ng, dcounts);
             pf.end(KF_PAIR_COUNTS, 8.0 * nmodes + 16.0 * nrep);
             k_counts_out<<<(ng + 127) / 128, 128, 0, c->stream>>>(ng, dcounts, didx + io, sumI);
             PS_CK(launch_status());

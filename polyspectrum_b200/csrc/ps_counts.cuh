@@ -24,7 +24,7 @@ namespace ps {
 // representatives of its orbits under the 48 axis permutations and sign
 // flips with their orbit sizes as weights: S_b, the closing shells and |w(.)|^2
 // are invariant under them.  The pairs are cut into work items (a chunk of
-// 256 BPT modes of S_b times a slice of rep_slice representatives); each CTA
+// THREADS BPT modes of S_b times a slice of rep_slice representatives); each CTA
 // of a grid of resident CTAs takes items blockIdx.x, + gridDim.x, ... into
 // its own histogram of |w(m_a + m_b)|^2 - s_lo over nbins bins in shared
 // memory (integer atomics: the result does not depend on their order), so
@@ -35,12 +35,13 @@ namespace ps {
 // negative value for the idle slots past nb), so a pair costs three
 // multiply-adds, an add and the range test before its atomic.
 constexpr int kCountBPT = 4;
+constexpr int kCountThreads = 1024;  // one CTA per SM: 32 warps to hide the atomics' latency
 constexpr int kCountRepChunk = 512;  // largest rep_slice
 constexpr size_t kCountStageBytes = kCountRepChunk * (sizeof(int4) + sizeof(int));
 constexpr int kCountMaxBins = 44 * 1024;  // 176 KB of uint32 bins beside the staged representatives
 
-template <bool WRAP, int BPT = kCountBPT>
-__global__ void __launch_bounds__(256)
+template <bool WRAP, int BPT = kCountBPT, int THREADS = kCountThreads>
+__global__ void __launch_bounds__(THREADS)
     k_pair_counts(const int4* __restrict__ reps, int nrep, const short4* __restrict__ modes, int nb, int n, int s_lo,
                   int nbins, int rep_slice, const Shell* __restrict__ closing, int ncl,
                   unsigned long long* __restrict__ counts)
@@ -51,7 +52,7 @@ __global__ void __launch_bounds__(256)
     unsigned int* hist = reinterpret_cast<unsigned int*>(smem_raw + kCountStageBytes);
     for (int i = threadIdx.x; i < nbins; i += blockDim.x) hist[i] = 0u;
     const int half = n >> 1;
-    constexpr int kChunk = 256 * BPT;
+    constexpr int kChunk = THREADS * BPT;
     rep_slice = max(1, min(rep_slice, kCountRepChunk));  // the staging buffer's size
     const int nmc = (nb + kChunk - 1) / kChunk, nrs = (nrep + rep_slice - 1) / rep_slice;
     const int nitems = nmc * nrs;
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(256)
         int bx[BPT], by[BPT], bz[BPT], bn[BPT];
 #pragma unroll
         for (int u = 0; u < BPT; u++) {
-            const int idx = mc * kChunk + u * 256 + (int)threadIdx.x;
+            const int idx = mc * kChunk + u * THREADS + (int)threadIdx.x;
             const bool valid = idx < nb;
             const short4 m = valid ? modes[idx] : short4{0, 0, 0, 0};
             bx[u] = m.x;

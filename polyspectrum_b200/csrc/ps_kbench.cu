@@ -157,22 +157,22 @@ double time_pair(int reps, const float2* wa, int Sa, int ba, const float2* wb, i
 // Mean time of `reps` launches of the exact-count kernel <WRAP, BPT> on the
 // lists L (closing shells dcl, ncl of them) with `grid` CTAs over work items
 // of rep_slice representatives; the counts of the last launch go to hc.
-template <bool WRAP, int BPT>
+template <bool WRAP, int BPT, int THREADS = kCountThreads>
 double time_counts(int reps, const PairCountLists& L, const int4* dreps, const short4* dmodes, int N,
                    const Shell* dcl, int ncl, unsigned long long* dcounts, int rep_slice, bool one_wave,
-                   std::vector<unsigned long long>& hc)
+                   std::vector<unsigned long long>& hc, bool max_ctas = false)
 {
     const int nrep = (int)L.reps.size(), nb = (int)L.modes.size();
     rep_slice = std::max(1, std::min(rep_slice, kCountRepChunk));
     const size_t smem = kCountStageBytes + (size_t)L.nbins * sizeof(unsigned int);
-    auto kern = k_pair_counts<WRAP, BPT>;
+    auto kern = k_pair_counts<WRAP, BPT, THREADS>;
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, sms = 0, per_sm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
-    const int nmc = (nb + 256 * BPT - 1) / (256 * BPT), nitems = nmc * ((nrep + rep_slice - 1) / rep_slice);
-    const int grid = one_wave ? std::min(nitems, std::max(per_sm, 1) * sms) : nitems;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem));
+    const int nmc = (nb + THREADS * BPT - 1) / (THREADS * BPT), nitems = nmc * ((nrep + rep_slice - 1) / rep_slice);
+    const int grid = one_wave ? std::min(nitems, max_ctas ? sms : std::max(per_sm, 1) * sms) : nitems;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -180,7 +180,7 @@ double time_counts(int reps, const PairCountLists& L, const int4* dreps, const s
     for (int it = 0; it < reps + 2; it++) {
         CK(cudaMemset(dcounts, 0, sizeof(unsigned long long) * ncl));
         CK(cudaEventRecord(e0));
-        kern<<<grid, 256, smem>>>(dreps, nrep, dmodes, nb, N, L.s_lo, L.nbins, rep_slice, dcl, ncl, dcounts);
+        kern<<<grid, THREADS, smem>>>(dreps, nrep, dmodes, nb, N, L.s_lo, L.nbins, rep_slice, dcl, ncl, dcounts);
         CK(cudaEventRecord(e1));
         CK(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -190,8 +190,9 @@ double time_counts(int reps, const PairCountLists& L, const int4* dreps, const s
     CK(cudaGetLastError());
     hc.assign(ncl, 0ull);
     CK(cudaMemcpy(hc.data(), dcounts, sizeof(unsigned long long) * ncl, cudaMemcpyDeviceToHost));
-    printf("pair_counts wrap=%d BPT=%d slice=%d %s: %.4f ms  (%d CTAs, %d CTAs/SM, %zu B smem)\n", (int)WRAP, BPT,
-           rep_slice, one_wave ? "one wave" : "one item per CTA", total / reps, grid, per_sm, smem);
+    printf("pair_counts wrap=%d BPT=%d threads=%d slice=%d %s: %.4f ms  (%d CTAs, %d CTAs/SM, %zu B smem)\n",
+           (int)WRAP, BPT, THREADS, rep_slice, one_wave ? (max_ctas ? "one CTA per SM" : "one wave") : "one item per CTA",
+           total / reps, grid, per_sm, smem);
     return total / reps;
 }
 struct Timer {
@@ -350,6 +351,14 @@ int main(int argc, char** argv)
         }
         time_counts<false, 1>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, 64, true, got); check(got);
         time_counts<false, 8>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, 64, true, got); check(got);
+        // one CTA per SM (the library's grid: the count lane beside the field lanes)
+        for (int slice : {32, 64, 128}) {
+            time_counts<false, 4, 256>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, slice, true, got, true); check(got);
+            time_counts<false, 4, 512>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, slice, true, got, true); check(got);
+            time_counts<false, 2, 512>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, slice, true, got, true); check(got);
+            time_counts<false, 4, 1024>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, slice, true, got, true); check(got);
+        }
+        time_counts<false, 4, 512>(reps, L, dreps, dmodes, NG, dcl, 16, dcnt, 64, true, got); check(got);
     }
     return 0;
 }
