@@ -761,9 +761,12 @@ enum SpecEpi : int {
 // instantiations so the storing pass is not sized for the sums' registers.
 // r2max (sums only): no shell of the launch holds a mode with |m|^2 > r2max,
 // so a tile of pencils whose (my, mz) lie outside that ball is skipped.
+// FP32 sums up to 384 points run two CTAs per SM (64 registers, a few bytes
+// of spill: the 384-point pass 0.149 against 0.165 ms at one CTA per SM).
 template <typename T, int N, bool DOT>
 __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
-                                  DOT ? (PencilGeom<T, N>::THREADS <= 256 ? 2 : 1) : (sizeof(T) == 8 ? 1 : 2))
+                                  DOT ? (((sizeof(T) == 4 && N <= 384) || PencilGeom<T, N>::THREADS <= 256) ? 2 : 1)
+                                      : (sizeof(T) == 8 ? 1 : 2))
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, int ndk, const Shell* __restrict__ shells,
             int nshell, const unsigned short* __restrict__ lut, int lut_size, double weight, int quad,
@@ -909,51 +912,56 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
             cp_async_wait_all();
             __syncthreads();
         }
-        double acc[MAX_DOT_SHELLS];
-#pragma unroll
-        for (int c = 0; c < MAX_DOT_SHELLS; c++) acc[c] = 0.0;
         // DOT sums carry `weight` (the (N_field / N)^3 of a sub-grid product spectrum)
         const double wgt =
             (double)(herm_weight(h, N) * (quad && j != 0 && j != N / 2 ? 2 : 1)) * (use_dk ? weight : 1.0);
         const double inv_n3 = 1.0 / ((double)N * (double)N * (double)N);
-#pragma unroll
-        for (int e = 0; e < G::R; e++) {
-            const unsigned b = (bits2[e / 2] >> (16 * (e & 1))) & 0xffffu;
-            if (b) {
-                double val;
-                if (use_dk) {
-                    V d;
-                    if constexpr (G::DK_SMEM) {
-                        d = sdk[(t + G::TPF * e) * G::W + w];
-                    } else {
-                        const int mx = lattice_freq(t + G::TPF * e, N);
-                        d = dk[((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h];
-                    }
-                    val = wgt * ((double)d.x * (double)a[e].x + (double)d.y * (double)a[e].y);
-                } else {
-                    val = wgt * rint((double)a[e].x * inv_n3);
-                }
-                if (epi == SPEC_DOT_ABS) val = fabs(val);
-#pragma unroll
-                for (int c = 0; c < MAX_DOT_SHELLS; c++)
-                    if ((b >> c) & 1u) acc[c] += val;
-            }
-        }
-        // warp sums of the 16 shells by recursive halving: at lane offset o
-        // each lane keeps half of its shells (the upper half when lane & o)
-        // and adds the partner's copy of that half, so after offsets 16, 8,
-        // 4, 2 lane l holds one shell, c(l) = 8 b4 + 4 b3 + 2 b2 + b1 (b_k
-        // the lane bits), summed over 16 lanes; offset 1 completes it.
-        static_assert(MAX_DOT_SHELLS == 16, "halving tree of 16 shells");
+        // the 16 shells in two halves of 8 (8 FP64 accumulators live at a
+        // time; a mode's term is formed once per half it has shells in).
+        // Warp sums of a half by recursive halving: at lane offset o each lane
+        // keeps half of its shells (the upper half when lane & o) and adds the
+        // partner's copy of that half, so after offsets 16, 8, 4 lane l holds
+        // shell c(l) = 4 b4 + 2 b3 + b2 of the half (b_k the lane bits), summed
+        // over 8 lanes; offsets 2 and 1 complete it.
+        static_assert(MAX_DOT_SHELLS == 16, "two halving trees of 8 shells");
         constexpr int NW = G::THREADS / 32;
         __shared__ double wsum[NW][MAX_DOT_SHELLS];
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        halve_sums<16, 16>(acc, lane);
-        halve_sums<8, 8>(acc, lane);
-        halve_sums<4, 4>(acc, lane);
-        halve_sums<2, 2>(acc, lane);
-        acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 1);
-        if ((lane & 1) == 0) wsum[wid][(lane >> 1) & 15] = acc[0];
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            double acc[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) acc[c] = 0.0;
+#pragma unroll
+            for (int e = 0; e < G::R; e++) {
+                const unsigned b = (bits2[e / 2] >> (16 * (e & 1) + 8 * half)) & 0xffu;
+                if (b) {
+                    double val;
+                    if (use_dk) {
+                        V d;
+                        if constexpr (G::DK_SMEM) {
+                            d = sdk[(t + G::TPF * e) * G::W + w];
+                        } else {
+                            const int mx = lattice_freq(t + G::TPF * e, N);
+                            d = dk[((size_t)(mx < 0 ? mx + ndk : mx) * ndk + jdk) * dk_stride + h];
+                        }
+                        val = wgt * ((double)d.x * (double)a[e].x + (double)d.y * (double)a[e].y);
+                    } else {
+                        val = wgt * rint((double)a[e].x * inv_n3);
+                    }
+                    if (epi == SPEC_DOT_ABS) val = fabs(val);
+#pragma unroll
+                    for (int c = 0; c < 8; c++)
+                        if ((b >> c) & 1u) acc[c] += val;
+                }
+            }
+            halve_sums<8, 16>(acc, lane);
+            halve_sums<4, 8>(acc, lane);
+            halve_sums<2, 4>(acc, lane);
+            acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 2);
+            acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 1);
+            if ((lane & 3) == 0) wsum[wid][8 * half + ((lane >> 2) & 7)] = acc[0];
+        }
         __syncthreads();
         if (threadIdx.x < nshell) {
             double sum = 0.0;
