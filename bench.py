@@ -570,6 +570,7 @@ def run_ours(args, rank, world, local_rank):
                                             f"of the results per step"),
                                configs_total=ncfg_total,
                                subgrids=[int(ln.split()[-1]) for ln in tune_table.splitlines() if ln.startswith("grid")],
+                               tune_table=[ln for ln in tune_table.splitlines() if ln.strip()],
                                spectrum_band=spectrum_band, value_full_spectrum=value_full),
                    e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=h2d,
                             d2h_bytes_per_step=d2h, ms_per_step=ms_e2e,

@@ -158,8 +158,11 @@ int ps_gpu_polyspectrum_batch(ps_gpu_ctx *ctx, int method, int nconf, ps_cfg *cf
  * flag the fastest of the smallest and up to two larger supported sizes, timed
  * at plan creation; the flag also times, per FP32 transform size the groups
  * use, the Y pass with its default thread layout against one with twice the
- * elements per thread (one radix pass fewer) and keeps the faster.  Counts
- * are identical either way; sums differ only by FP32 rounding.  Choices are
+ * elements per thread (one radix pass fewer) and keeps the faster, and the
+ * pair kernel (the per-row product of two inverse transforms, transformed
+ * forward again) in its default layout, with one row transform live in
+ * registers, and with twice the elements per thread, keeping the fastest.
+ * Counts are identical either way; sums differ only by FP32 rounding.  Choices are
  * kept per context and can be exported / imported (ps_gpu_tune_export /
  * ps_gpu_tune_import) so later runs use the same sizes and layouts. */
 #define PS_PLAN_AUTOTUNE 4
@@ -257,8 +260,11 @@ int ps_gpu_plan_results(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *B, double *N
 int ps_gpu_plan_results_device(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *dst);
 
 /* The context's autotuned choices as text, one "grid N b_a b_b b_c M" line per
- * pair-group signature and one "pencil M alt" line (alt 0 or 1) per transform
- * size whose Y pass layout was timed: writes at most buflen bytes (NUL-terminated) and
+ * pair-group signature, one "pencil M alt" line (alt 0 or 1) per transform
+ * size whose Y pass layout was timed and one "pair M v" line per FP32
+ * transform size whose pair kernel variant was timed (v 0: the default, 1: one
+ * row transform live in registers, 2: twice the elements per thread, one
+ * radix pass fewer): writes at most buflen bytes (NUL-terminated) and
  * returns the length of the whole text, or a negative status.  Import adds
  * the lines of such a text to the context's choices (unknown or malformed
  * lines: PS_ERR_ARG, nothing imported).  No reference counterpart. */

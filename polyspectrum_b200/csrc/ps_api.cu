@@ -150,7 +150,8 @@ template <typename T> struct PrecBufs {
     V2<T>* twp = nullptr;   // Stockham table of the pencil transforms (length N)
     V2<T>* twr = nullptr;   // Stockham table of the row transforms (length N/2)
     V2<T>* twp_alt = nullptr;  // table of the alternative Y pass (PencilAlt), if N has one
-    Tables<T> tables() const { return Tables<T>{twp, twr, tw, twp_alt}; }
+    V2<T>* twr_alt = nullptr;  // row table of pair kernel variant 2 (PairVariants::ALT_RX), if N has one
+    Tables<T> tables() const { return Tables<T>{twp, twr, tw, twp_alt, twr_alt}; }
     V2<T>* spec = nullptr;  // field spectrum, row stride S
     V2<T>* work = nullptr;  // work spectrum (band-limited strides <= S)
     V2<T>* work2 = nullptr; // second and third work spectra (pair groups; allocated on use)
@@ -163,7 +164,7 @@ template <typename T> struct PrecBufs {
     bool have_spec = false;
     bool have_mod = false;
     // tables of smaller transform sizes (sub-grid products), made at plan time
-    std::map<int, std::array<V2<T>*, 4>> sub;
+    std::map<int, std::array<V2<T>*, 5>> sub;
 };
 
 // Host worker threads of the composition, one pool per process shared by
@@ -298,6 +299,9 @@ struct ps_gpu_ctx {
     // autotuned Y pass geometry per FP32 transform size: 1 = the alternative
     // (PencilAlt: twice the elements per thread), 0 = the default
     std::map<int, int> pencil_alt;
+    // autotuned pair kernel variant per FP32 transform size (PairVariants:
+    // 0 the default, 1 one live row transform, 2 twice the elements per thread)
+    std::map<int, int> pair_var;
     bool capturing = false;  // inside a plan graph capture: no profiling events
     // host uploads: two staging slots of (dens, xhii), filled on copy_stream;
     // ev_copied[s] = slot s filled, ev_free[s] = its forward transform is done
@@ -431,6 +435,12 @@ template <typename T> int init_prec(ps_gpu_ctx* c, PrecBufs<T>& b)
             PS_TRY(alloc_dev(&b.twp_alt, N));
             PS_CK(cudaMemcpy(b.twp_alt, ha.data(), sizeof(V2<T>) * N, cudaMemcpyHostToDevice));
         }
+        bool has_pair_alt = false;
+        PS_SWITCH_N(N, (has_pair_alt = L3<T, NN>::host_pair_alt_table(hr.data())));
+        if (has_pair_alt) {
+            PS_TRY(alloc_dev(&b.twr_alt, N / 2));
+            PS_CK(cudaMemcpy(b.twr_alt, hr.data(), sizeof(V2<T>) * (N / 2), cudaMemcpyHostToDevice));
+        }
     }
     PS_TRY(alloc_dev(&b.spec, nspec));
     PS_TRY(alloc_dev(&b.work, nspec));
@@ -461,12 +471,13 @@ template <typename T> int tables_for(ps_gpu_ctx* c, int M, Tables<T>* out)
     auto it = b.sub.find(M);
     if (it == b.sub.end()) {
         if (c->capturing) return fail(PS_ERR_ARG, "internal: tables of size %d not made before capture", M);
-        std::array<V2<T>*, 4> t = {nullptr, nullptr, nullptr, nullptr};
-        std::vector<V2<T>> hp(M), hr(M / 2), h(M), ha(M);
+        std::array<V2<T>*, 5> t = {nullptr, nullptr, nullptr, nullptr, nullptr};
+        std::vector<V2<T>> hp(M), hr(M / 2), h(M), ha(M), hr2(M / 2);
         const int N = M;
         PS_SWITCH_N(N, (L3<T, NN>::host_tables(hp.data(), hr.data())));
-        bool has_alt = false;
+        bool has_alt = false, has_pair_alt = false;
         PS_SWITCH_N(N, (has_alt = L3<T, NN>::host_alt_table(ha.data())));
+        PS_SWITCH_N(N, (has_pair_alt = L3<T, NN>::host_pair_alt_table(hr2.data())));
         const long double two_pi = 6.283185307179586476925286766559005768L;
         for (int m = 0; m < M; m++) {
             const long double a = two_pi * (long double)m / (long double)M;
@@ -477,6 +488,7 @@ template <typename T> int tables_for(ps_gpu_ctx* c, int M, Tables<T>* out)
         if (rc == PS_OK) rc = alloc_dev(&t[1], M / 2);
         if (rc == PS_OK) rc = alloc_dev(&t[2], M);
         if (rc == PS_OK && has_alt) rc = alloc_dev(&t[3], M);
+        if (rc == PS_OK && has_pair_alt) rc = alloc_dev(&t[4], M / 2);
         if (rc != PS_OK) {
             for (V2<T>* p : t) cudaFree(p);
             return rc;
@@ -486,9 +498,10 @@ template <typename T> int tables_for(ps_gpu_ctx* c, int M, Tables<T>* out)
         PS_CK(cudaMemcpy(t[1], hr.data(), sizeof(V2<T>) * (M / 2), cudaMemcpyHostToDevice));
         PS_CK(cudaMemcpy(t[2], h.data(), sizeof(V2<T>) * M, cudaMemcpyHostToDevice));
         if (has_alt) PS_CK(cudaMemcpy(t[3], ha.data(), sizeof(V2<T>) * M, cudaMemcpyHostToDevice));
+        if (has_pair_alt) PS_CK(cudaMemcpy(t[4], hr2.data(), sizeof(V2<T>) * (M / 2), cudaMemcpyHostToDevice));
         it = b.sub.find(M);
     }
-    *out = Tables<T>{it->second[0], it->second[1], it->second[2], it->second[3]};
+    *out = Tables<T>{it->second[0], it->second[1], it->second[2], it->second[3], it->second[4]};
     return PS_OK;
 }
 
@@ -501,6 +514,7 @@ template <typename T> void free_prec(PrecBufs<T>& b)
     cudaFree(b.twp);
     cudaFree(b.twr);
     cudaFree(b.twp_alt);
+    cudaFree(b.twr_alt);
     cudaFree(b.spec);
     cudaFree(b.work);
     cudaFree(b.work2);
@@ -641,6 +655,14 @@ template <typename T> int pencil_alt_of(const ps_gpu_ctx* c, int M)
     if (sizeof(T) != 4) return 0;
     const auto it = c->pencil_alt.find(M);
     return it == c->pencil_alt.end() ? 0 : it->second;
+}
+
+// Pair kernel variant of an M-point transform of precision T (autotuned choice).
+template <typename T> int pair_var_of(const ps_gpu_ctx* c, int M)
+{
+    if (sizeof(T) != 4) return 0;
+    const auto it = c->pair_var.find(M);
+    return it == c->pair_var.end() ? 0 : it->second;
 }
 
 }  // namespace
@@ -803,7 +825,8 @@ int pair_spectrum(ps_gpu_ctx* c, const V2<T>* A, int Sa, int hba, const V2<T>* B
     const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / NN2 : 1.0;
     {
         Prof pf(c);
-        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, tb, quad))));
+        PS_SWITCH_N(N, PS_TRY((L3<T, NN>::pair_z(c->stream, A, Sa, hba, Bq, Sb, hbb, B.work3, S, hout, tb, quad,
+                                                 pair_var_of<T>(c, N)))));
         pf.end(fam<T>(KF_PAIR_Z), q * NN2 * (hba + (Bq ? hbb : 0) + hout) * V, N);
     }
     {
@@ -1560,6 +1583,66 @@ int tune_pencil(ps_gpu_ctx* c, int M)
     return rc;
 }
 
+// Autotuning of the FP32 pair kernel variant of an M-point transform
+// (PairVariants: the default, one live row transform, twice the elements per
+// thread): every variant the length has runs once to warm up, then three times
+// timed with CUDA events, on legs of hva / hvb valid columns (hvb = 0: one leg
+// squared) read from the start of a scratch work spectrum and products of hout
+// columns written behind them; the fastest is kept for the context.  The
+// variants compute the same transforms (their sums differ by FP32 rounding).
+int tune_pair(ps_gpu_ctx* c, int M, int hva, int hvb, int hout)
+{
+    if (c->pair_var.count(M)) return PS_OK;
+    int mask = 1;
+    {
+        const int N = M;
+        PS_SWITCH_N(N, (mask = L3<float, NN>::pair_variants()));
+    }
+    const int w = pw<float>(M);
+    const int Sa = round_up(std::max(hva, hvb), w), Sd = round_up(hout, w);
+    const size_t need = (size_t)M * M * (size_t)(Sa + Sd);
+    if (mask == 1 || !c->f.work || need > (size_t)c->N * c->N * c->f.S) {
+        c->pair_var[M] = 0;
+        return PS_OK;
+    }
+    Tables<float> tb;
+    PS_TRY(tables_for<float>(c, M, &tb));
+    const V2<float>* src = c->f.work;
+    V2<float>* dst = c->f.work + (size_t)M * M * Sa;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PS_CK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(PS_ERR_CUDA, "event creation failed");
+    }
+    float best_ms = 0.f;
+    int best = 0, rc = PS_OK;
+    for (int v = 0; v < 3 && rc == PS_OK; v++) {
+        if (!((mask >> v) & 1)) continue;
+        const int N = M;
+        auto run = [&]() -> int {
+            PS_SWITCH_N(N, PS_TRY((L3<float, NN>::pair_z(c->stream, src, Sa, hva, hvb > 0 ? src : nullptr, Sa, hvb,
+                                                         dst, Sd, hout, tb, 0, v))));
+            return PS_OK;
+        };
+        if ((rc = run()) != PS_OK) break;
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 3 && rc == PS_OK; r++) rc = run();
+        cudaEventRecord(e1, c->stream);
+        if (rc == PS_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = fail(PS_ERR_CUDA, "autotune timing failed");
+        float ms = 0.f;
+        if (rc == PS_OK) cudaEventElapsedTime(&ms, e0, e1);
+        if (rc == PS_OK && (v == 0 || ms < best_ms)) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == PS_OK) c->pair_var[M] = best;
+    return rc;
+}
+
 int sum_partials_n(ps_gpu_ctx* c, int nblocks, int ncols, double* out)
 {
     return sum_partials(c, nblocks, ncols, out, 1);
@@ -2000,6 +2083,9 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             PS_TRY(tables_for<float>(c, M, &t32));
             PS_TRY(tables_for<double>(c, M, &t64));
         }
+        if (P->flags & PS_PLAN_AUTOTUNE)  // the FP32 pair kernel variant of this transform size
+            PS_TRY(tune_pair(c, M, std::min(sa.band, M / 2) + 1, G.a != G.b ? std::min(sb.band, M / 2) + 1 : 0,
+                             hout));
         group_dop[g] = d_part(M);
         group_iop[g] = i_part(M);
         group_M[g] = M;
@@ -3402,6 +3488,10 @@ int ps_gpu_tune_export(ps_gpu_ctx* c, char* buf, int buflen)
         snprintf(line, sizeof(line), "pencil %d %d\n", kv.first, kv.second);
         t += line;
     }
+    for (const auto& kv : c->pair_var) {
+        snprintf(line, sizeof(line), "pair %d %d\n", kv.first, kv.second);
+        t += line;
+    }
     if (buf && buflen > 0) {
         const size_t n = std::min(t.size(), (size_t)buflen - 1);
         memcpy(buf, t.data(), n);
@@ -3415,7 +3505,7 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
     g_err[0] = 0;
     if (!c || !text) return fail(PS_ERR_ARG, "NULL argument");
     std::map<std::array<int, 4>, int> add;
-    std::map<int, int> add_pencil;
+    std::map<int, int> add_pencil, add_pair;
     const char* p = text;
     while (*p) {
         const char* e = strchr(p, '\n');
@@ -3431,6 +3521,14 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
             continue;
         }
         used = 0;
+        if (sscanf(ln.c_str(), "pair %d %d %n", &m, &n, &used) == 2 &&
+            ln.find_first_not_of(" \t\r", used) == std::string::npos) {
+            if (!grid_size_ok(m) || n < 0 || n > 2)
+                return fail(PS_ERR_ARG, "tune line out of range: '%s'", ln.c_str());
+            add_pair[m] = n;
+            continue;
+        }
+        used = 0;
         if (sscanf(ln.c_str(), "grid %d %d %d %d %d %n", &n, &ba, &bb, &bc, &m, &used) != 5 ||
             ln.find_first_not_of(" \t\r", used) != std::string::npos)
             return fail(PS_ERR_ARG, "tune line not understood: '%s'", ln.c_str());
@@ -3440,6 +3538,7 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
     }
     for (const auto& kv : add) c->tune_grid[kv.first] = kv.second;
     for (const auto& kv : add_pencil) c->pencil_alt[kv.first] = kv.second;
+    for (const auto& kv : add_pair) c->pair_var[kv.first] = kv.second;
     return PS_OK;
 }
 

@@ -676,6 +676,19 @@ template <typename T, int N, int RX, bool KEEP> struct PairGeom {
     {
         return G::smem(ninputs, hva, hvb) + (KEEP ? (size_t)G::WZ * G::ROWBUF * sizeof(V2<T>) : 0);
     }
+    static constexpr bool FITS = smem(2, N / 2 + 1, N / 2 + 1) <= 227 * 1024;
+};
+
+// Pair kernel variants the plan autotuner times per FP32 transform size of
+// register-plan rows from 128 to 512 points: 0 the default, 1 KEEP (one row
+// transform live in registers), 2 KEEP with twice the default elements per
+// thread (one radix pass fewer, half the threads per row).  KEEP_OK /
+// ALT_RX (0: none) say which exist for a length.
+template <typename T, int N> struct PairVariants {
+    static constexpr bool REG = sizeof(T) == 4 && !LenKind<N / 2>::RAGGED && N >= 128 && N <= 512;
+    static constexpr int RX2 = 2 * RowGeom<T, N>::R;
+    static constexpr bool KEEP_OK = REG && PairGeom<T, N, 0, true>::FITS;
+    static constexpr int ALT_RX = REG && (N / 2) % RX2 == 0 && (N / 2) / RX2 >= 4 ? RX2 : 0;
 };
 
 template <typename T, int N, int RX = 0, bool KEEP = false>

@@ -59,6 +59,7 @@ template <typename T> struct Tables {
     const V2<T>* twr;
     const V2<T>* twpp;
     const V2<T>* twp_alt = nullptr;  // Stockham table of the alternative Y pass (PencilAlt), if any
+    const V2<T>* twr_alt = nullptr;  // row table of pair kernel variant 2 (PairVariants::ALT_RX), if any
 };
 
 template <typename T, int N> struct L3 {
@@ -78,6 +79,29 @@ template <typename T, int N> struct L3 {
             (void)twp_alt;
             return false;
         }
+    }
+    static constexpr int PAIR_RX2 = PairVariants<T, N>::ALT_RX;
+    // host copy of the row table of pair kernel variant 2 (false: no such variant)
+    static bool host_pair_alt_table(V* twr_alt)
+    {
+        if constexpr (PAIR_RX2 > 0) {
+            using G2 = RowGeom<T, N, PAIR_RX2>;
+            transform_table<V, N / 2, G2::R, G2::TPF>(twr_alt);
+            return true;
+        } else {
+            (void)twr_alt;
+            return false;
+        }
+    }
+    // the pair kernel variants this length has (PairVariants): bit v set = variant v runs
+    static int pair_variants()
+    {
+        int m = 1;
+        if constexpr (PairVariants<T, N>::KEEP_OK) m |= 2;
+        if constexpr (PAIR_RX2 > 0) {
+            if constexpr (PairGeom<T, N, PAIR_RX2, true>::FITS) m |= 4;
+        }
+        return m;
     }
     // host copies of the tables for this N
     static void host_tables(V* twp, V* twr)
@@ -181,17 +205,38 @@ template <typename T, int N> struct L3 {
         k_fwd_z<T, N, false><<<blocks, RG::THREADS, smem, st>>>(kind, a, b, dst, ds, hout, vec, tb.twr, tb.twpp);
         return PS_OK;
     }
-    static int pair_z(cudaStream_t st, const V* a, int sa, int hva, const V* b, int sb, int hvb, V* dst,
-                      int ds, int hout, const Tables<T>& tb, int quad = 0)
+    template <int RX, bool KEEP>
+    static int pair_z_v(cudaStream_t st, const V* a, int sa, int hva, const V* b, int sb, int hvb, V* dst, int ds,
+                        int hout, const V* twr, const V* twpp, int quad)
     {
-        const size_t smem = RG::smem(b ? 2 : 1, hva, hvb);
-        PS_LTRY(set_smem(k_pair_z<T, N>, RG::smem(2, N / 2 + 1, N / 2 + 1)));
+        using G = RowGeom<T, N, RX>;
+        using PGm = PairGeom<T, N, RX, KEEP>;
+        const size_t smem = PGm::smem(b ? 2 : 1, hva, hvb);
+        PS_LTRY(set_smem(k_pair_z<T, N, RX, KEEP>, PGm::smem(2, N / 2 + 1, N / 2 + 1)));
         const int nrows = quad ? (N / 2 + 1) * (N / 2 + 1) : N * N;
         int grid = 0;
-        PS_LTRY(persistent_grid(k_pair_z<T, N>, RG::THREADS, smem, (nrows + RG::WZ - 1) / RG::WZ, &grid));
-        k_pair_z<T, N><<<grid, RG::THREADS, smem, st>>>(a, sa, hva, b, sb, hvb, dst, ds, hout, nrows, tb.twr,
-                                                        tb.twpp);
+        PS_LTRY(persistent_grid(k_pair_z<T, N, RX, KEEP>, G::THREADS, smem, (nrows + G::WZ - 1) / G::WZ, &grid));
+        k_pair_z<T, N, RX, KEEP><<<grid, G::THREADS, smem, st>>>(a, sa, hva, b, sb, hvb, dst, ds, hout, nrows, twr,
+                                                                 twpp);
         return PS_OK;
+    }
+    // variant: the autotuned pair kernel variant (PairVariants; 0 the default,
+    // and the default wherever the length lacks the one asked for)
+    static int pair_z(cudaStream_t st, const V* a, int sa, int hva, const V* b, int sb, int hvb, V* dst,
+                      int ds, int hout, const Tables<T>& tb, int quad = 0, int variant = 0)
+    {
+        if constexpr (PAIR_RX2 > 0) {
+            if constexpr (PairGeom<T, N, PAIR_RX2, true>::FITS) {
+                if (variant == 2 && tb.twr_alt && !quad)
+                    return pair_z_v<PAIR_RX2, true>(st, a, sa, hva, b, sb, hvb, dst, ds, hout, tb.twr_alt, tb.twpp,
+                                                    quad);
+            }
+        }
+        if constexpr (PairVariants<T, N>::KEEP_OK) {
+            if (variant == 1 && !quad)
+                return pair_z_v<0, true>(st, a, sa, hva, b, sb, hvb, dst, ds, hout, tb.twr, tb.twpp, quad);
+        }
+        return pair_z_v<0, false>(st, a, sa, hva, b, sb, hvb, dst, ds, hout, tb.twr, tb.twpp, quad);
     }
     // ndk: grid size of the field spectrum dk (0: N); r2max: bound of the
     // launch's shells' |m|^2 for the sum epilogues (tiles outside are skipped)

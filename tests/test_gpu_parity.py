@@ -419,6 +419,7 @@ def test_autotuned_plan_and_tune_table(gpu_lib):
         table = ctx.tune_export()
     assert table.count("grid ") >= 2, table
     assert "pencil " in table, table  # the Y pass geometry per transform size
+    assert "pair " in table, table  # the pair kernel variant per transform size
     scale = np.abs(B64).max()
     assert np.all(np.abs(Bt - B64) <= 1e-5 * np.abs(B64) + 1e-6 * scale)
     np.testing.assert_array_equal(Nt, np.rint(N64))
@@ -435,6 +436,49 @@ def test_autotuned_plan_and_tune_table(gpu_lib):
             ctx2.tune_import("grid 256 1 2 three 64\n")
     np.testing.assert_array_equal(B2, Bt)
     np.testing.assert_array_equal(N2, Nt)
+
+
+def test_pair_kernel_variants_from_tune_table(gpu_lib):
+    """Every pair kernel variant the autotuner chooses from (0 the default,
+    1 one live row transform, 2 twice the elements per thread), forced through
+    an imported tune table on 128-, 192- and 256-point sub-grids, keeps counts
+    and derived ranges identical and B within the batched tolerance of plain
+    FP64; a table naming a variant outside 0..2 is refused."""
+    from polyspectrum_b200 import synth
+    ps = gpu_lib
+    n_grid, box = 256, 400.0
+    dens, xhii = synth.xhi_dens_inputs(n_grid, box, 4000, 3, 2.0, 4)
+    cfgs = []
+    for k1, k2 in ((0.2, 0.5), (0.5, 0.8), (0.8, 1.2)):
+        c, _, _ = ps.read_params_to_kvectors(n_grid, box, 3, k1=k1, k2=k2, num_values=6, kbinningCase=1)
+        cfgs += [c[i] for i in range(len(c))]
+    with ps.Context(n_grid, box) as ctx:
+        ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+        plan = ctx.plan(cfgs, autotune=True)
+        plan.close()
+        grids = [ln.split() for ln in ctx.tune_export().splitlines() if ln.startswith("grid ")]
+        B64, N64, _, out64 = ctx.batch(cfgs, ps.PS_FP64_PLAIN)
+    assert grids
+    scale = np.abs(B64).max()
+    for M in (128, 192, 256):
+        table = "".join(f"grid {g[1]} {g[2]} {g[3]} {g[4]} {max(M, int(g[5]))}\n" for g in grids)
+        for v in (0, 1, 2):
+            with ps.Context(n_grid, box) as ctx:
+                ctx.tune_import(table + "".join(f"pair {m} {v}\n" for m in (128, 192, 256)))
+                assert f"pair {M} {v}" in ctx.tune_export()
+                ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
+                plan = ctx.plan(cfgs)
+                Bv, Nv, _, outv = plan.execute()
+                plan.close()
+            err = np.abs(Bv - B64)
+            assert np.all(err <= 1e-5 * np.abs(B64) + 1e-6 * scale), (M, v, err.max())
+            np.testing.assert_array_equal(Nv, np.rint(N64))
+            for i in range(len(cfgs)):
+                assert list(outv[i].kmin)[:3] == list(out64[i].kmin)[:3]
+                assert list(outv[i].kmax)[:3] == list(out64[i].kmax)[:3]
+    with ps.Context(n_grid, box) as ctx:
+        with pytest.raises(ps.PsError):
+            ctx.tune_import("pair 256 3\n")
 
 
 @pytest.mark.parametrize("legs", [(3.1, 4.2, 3.7, 5.0), (4.0, 4.0, 4.0, 4.0), (2.9, 3.6, 4.4, 3.1, 5.2)],
