@@ -161,7 +161,9 @@ int ps_gpu_polyspectrum_batch(ps_gpu_ctx *ctx, int method, int nconf, ps_cfg *cf
  * elements per thread (one radix pass fewer) and keeps the faster, and the
  * pair kernel (the per-row product of two inverse transforms, transformed
  * forward again) in its default layout, with one row transform live in
- * registers, and with twice the elements per thread, keeping the fastest.
+ * registers, and with twice the elements per thread, keeping the fastest,
+ * and the 16-shell dot pass in its default geometry against twice the
+ * elements per thread (timed on the group's whole field part).
  * Counts are identical either way; sums differ only by FP32 rounding.  Choices are
  * kept per context and can be exported / imported (ps_gpu_tune_export /
  * ps_gpu_tune_import) so later runs use the same sizes and layouts. */
@@ -264,7 +266,9 @@ int ps_gpu_plan_results_device(ps_gpu_ctx *ctx, ps_gpu_plan *plan, double *dst);
  * size whose Y pass layout was timed and one "pair M v" line per FP32
  * transform size whose pair kernel variant was timed (v 0: the default, 1: one
  * row transform live in registers, 2: twice the elements per thread, one
- * radix pass fewer): writes at most buflen bytes (NUL-terminated) and
+ * radix pass fewer) and one "dot M alt" line per FP32 transform size whose
+ * dot pass geometry was timed (alt 1: twice the elements per thread): writes
+ * at most buflen bytes (NUL-terminated) and
  * returns the length of the whole text, or a negative status.  Import adds
  * the lines of such a text to the context's choices (unknown or malformed
  * lines: PS_ERR_ARG, nothing imported).  No reference counterpart. */

@@ -302,6 +302,8 @@ struct ps_gpu_ctx {
     // autotuned pair kernel variant per FP32 transform size (PairVariants:
     // 0 the default, 1 one live row transform, 2 twice the elements per thread)
     std::map<int, int> pair_var;
+    // autotuned FP32 dot pass geometry per transform size: 1 = PencilAlt
+    std::map<int, int> dot_alt;
     bool capturing = false;  // inside a plan graph capture: no profiling events
     // host uploads: two staging slots of (dens, xhii), filled on copy_stream;
     // ev_copied[s] = slot s filled, ev_free[s] = its forward transform is done
@@ -657,6 +659,14 @@ template <typename T> int pencil_alt_of(const ps_gpu_ctx* c, int M)
     return it == c->pencil_alt.end() ? 0 : it->second;
 }
 
+// Dot pass geometry of an M-point transform of precision T (autotuned choice).
+template <typename T> int dot_alt_of(const ps_gpu_ctx* c, int M)
+{
+    if (sizeof(T) != 4) return 0;
+    const auto it = c->dot_alt.find(M);
+    return it == c->dot_alt.end() ? 0 : it->second;
+}
+
 // Pair kernel variant of an M-point transform of precision T (autotuned choice).
 template <typename T> int pair_var_of(const ps_gpu_ctx* c, int M)
 {
@@ -966,7 +976,8 @@ int dot_pass(ps_gpu_ctx* c, V2<T>* data, int epi, int S, int hvalid, const Shell
             Prof pf(c);
             PS_SWITCH_N(N, PS_TRY((L3<T, NN>::fwd_x(c->stream, data, S, hvalid, epi, nullptr, 0, B.spec, B.S,
                                                     dshells + s0, cnt, lut, lut_size, c->partials, tb, &nb,
-                                                    weight, quad, c->N, (int)std::min<long long>(r2max, 0x7fffffff)))));
+                                                    weight, quad, c->N, (int)std::min<long long>(r2max, 0x7fffffff),
+                                                    nullptr, 0, NN, dot_alt_of<T>(c, N)))));
             const double q = quad ? (double)(N / 2 + 1) * (N / 2 + 1) / ((double)N * N) : 1.0;
             pf.end(fam<T>(KF_FWD_X_DOT), q * N * N * hvalid * sizeof(V2<T>) * (epi == SPEC_DOT ? 2.0 : 1.0), N);
         }
@@ -1643,6 +1654,48 @@ int tune_pair(ps_gpu_ctx* c, int M, int hva, int hvb, int hout)
     return rc;
 }
 
+// Autotuning of the FP32 dot pass geometry of an M-point transform (the
+// default against PencilAlt, twice the elements per thread): the group's
+// whole field part (masked inverse transforms, pair kernel, forward Y pass,
+// dot pass) runs once to warm up and three times timed with CUDA events in
+// each geometry; the faster is kept for the context.  Both give the same sums
+// up to FP32 rounding.
+int tune_dot(ps_gpu_ctx* c, const std::function<int()>& group_field_op, int M)
+{
+    if (c->dot_alt.count(M)) return PS_OK;
+    bool has_alt = false;
+    {
+        const int N = M;
+        PS_SWITCH_N(N, (has_alt = L3<float, NN>::ALT > 0));
+    }
+    if (!has_alt) {
+        c->dot_alt[M] = 0;
+        return PS_OK;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PS_CK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(PS_ERR_CUDA, "event creation failed");
+    }
+    float ms[2] = {0.f, 0.f};
+    int rc = PS_OK;
+    for (int alt = 0; alt < 2 && rc == PS_OK; alt++) {
+        c->dot_alt[M] = alt;
+        if ((rc = group_field_op()) != PS_OK) break;
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 3 && rc == PS_OK; r++) rc = group_field_op();
+        cudaEventRecord(e1, c->stream);
+        if (rc == PS_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = fail(PS_ERR_CUDA, "autotune timing failed");
+        if (rc == PS_OK) cudaEventElapsedTime(&ms[alt], e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc == PS_OK) c->dot_alt[M] = ms[1] < ms[0] ? 1 : 0;
+    else c->dot_alt.erase(M);
+    return rc;
+}
+
 int sum_partials_n(ps_gpu_ctx* c, int nblocks, int ncols, double* out)
 {
     return sum_partials(c, nblocks, ncols, out, 1);
@@ -2083,9 +2136,17 @@ int plan_batched(ps_gpu_ctx* c, ps_gpu_plan* P)
             PS_TRY(tables_for<float>(c, M, &t32));
             PS_TRY(tables_for<double>(c, M, &t64));
         }
-        if (P->flags & PS_PLAN_AUTOTUNE)  // the FP32 pair kernel variant of this transform size
+        if (P->flags & PS_PLAN_AUTOTUNE) {  // the FP32 pair kernel variant and dot pass geometry of this size
             PS_TRY(tune_pair(c, M, std::min(sa.band, M / 2) + 1, G.a != G.b ? std::min(sb.band, M / 2) + 1 : 0,
                              hout));
+            if (!c->dot_alt.count(M)) {
+                if (!prefix_done) {  // the DERIVED chain fills the closing shells the group reads
+                    for (auto& op : ops) PS_TRY(op());
+                    prefix_done = true;
+                }
+                PS_TRY(tune_dot(c, d_part(M), M));
+            }
+        }
         group_dop[g] = d_part(M);
         group_iop[g] = i_part(M);
         group_M[g] = M;
@@ -3492,6 +3553,10 @@ int ps_gpu_tune_export(ps_gpu_ctx* c, char* buf, int buflen)
         snprintf(line, sizeof(line), "pair %d %d\n", kv.first, kv.second);
         t += line;
     }
+    for (const auto& kv : c->dot_alt) {
+        snprintf(line, sizeof(line), "dot %d %d\n", kv.first, kv.second);
+        t += line;
+    }
     if (buf && buflen > 0) {
         const size_t n = std::min(t.size(), (size_t)buflen - 1);
         memcpy(buf, t.data(), n);
@@ -3505,7 +3570,7 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
     g_err[0] = 0;
     if (!c || !text) return fail(PS_ERR_ARG, "NULL argument");
     std::map<std::array<int, 4>, int> add;
-    std::map<int, int> add_pencil, add_pair;
+    std::map<int, int> add_pencil, add_pair, add_dot;
     const char* p = text;
     while (*p) {
         const char* e = strchr(p, '\n');
@@ -3529,6 +3594,14 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
             continue;
         }
         used = 0;
+        if (sscanf(ln.c_str(), "dot %d %d %n", &m, &n, &used) == 2 &&
+            ln.find_first_not_of(" \t\r", used) == std::string::npos) {
+            if (!grid_size_ok(m) || (n != 0 && n != 1))
+                return fail(PS_ERR_ARG, "tune line out of range: '%s'", ln.c_str());
+            add_dot[m] = n;
+            continue;
+        }
+        used = 0;
         if (sscanf(ln.c_str(), "grid %d %d %d %d %d %n", &n, &ba, &bb, &bc, &m, &used) != 5 ||
             ln.find_first_not_of(" \t\r", used) != std::string::npos)
             return fail(PS_ERR_ARG, "tune line not understood: '%s'", ln.c_str());
@@ -3539,6 +3612,7 @@ int ps_gpu_tune_import(ps_gpu_ctx* c, const char* text)
     for (const auto& kv : add) c->tune_grid[kv.first] = kv.second;
     for (const auto& kv : add_pencil) c->pencil_alt[kv.first] = kv.second;
     for (const auto& kv : add_pair) c->pair_var[kv.first] = kv.second;
+    for (const auto& kv : add_dot) c->dot_alt[kv.first] = kv.second;
     return PS_OK;
 }
 

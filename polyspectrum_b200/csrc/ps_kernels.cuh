@@ -776,9 +776,11 @@ enum SpecEpi : int {
 // so a tile of pencils whose (my, mz) lie outside that ball is skipped.
 // FP32 sums up to 384 points run two CTAs per SM (64 registers, a few bytes
 // of spill: the 384-point pass 0.149 against 0.165 ms at one CTA per SM).
-template <typename T, int N, bool DOT>
-__global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
-                                  DOT ? (((sizeof(T) == 4 && N <= 384) || PencilGeom<T, N>::THREADS <= 256) ? 2 : 1)
+// RX > 0 (FP32 dot passes, autotuned): the alternative pencil geometry of
+// PencilAlt, twice the elements per thread and one radix pass fewer.
+template <typename T, int N, bool DOT, int RX = 0>
+__global__ void __launch_bounds__(PencilGeom<T, N, RX>::THREADS,
+                                  DOT ? (((sizeof(T) == 4 && N <= 384) || PencilGeom<T, N, RX>::THREADS <= 256) ? 2 : 1)
                                       : (sizeof(T) == 8 ? 1 : 2))
     k_fwd_x(V2<T>* data, int stride, int hvalid, int epi, V2<T>* out, int out_stride,
             const V2<T>* __restrict__ dk, int dk_stride, int ndk, const Shell* __restrict__ shells,
@@ -786,7 +788,7 @@ __global__ void __launch_bounds__(PencilGeom<T, N>::THREADS,
             int r2max, double* __restrict__ partials, const V2<T>* __restrict__ tw_g, T* __restrict__ mod_out,
             int ncols, int jband)
 {
-    using G = PencilGeom<T, N>;
+    using G = PencilGeom<T, N, RX>;
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int w = threadIdx.x % G::W, t = threadIdx.x / G::W;

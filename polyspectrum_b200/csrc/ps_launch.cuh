@@ -244,12 +244,23 @@ template <typename T, int N> struct L3 {
                      const V* dk, int dks, const Shell* shells, int nshell, const unsigned short* lut,
                      int lut_size, double* partials, const Tables<T>& tb, int* nblocks, double weight = 1.0,
                      int quad = 0, int ndk = 0, int r2max = 0x7fffffff, T* mod_out = nullptr, int ncols = 0,
-                     int jband = N)
+                     int jband = N, int alt = 0)
     {
         const int nj = quad ? N / 2 + 1 : N;
         const int nc = ncols > 0 ? ncols : stride;
         const unsigned blocks = (unsigned)(nj * (nc / PG::W));
         const bool dot = epi == SPEC_DOT || epi == SPEC_COUNT || epi == SPEC_DOT_ABS;
+        if constexpr (ALT > 0) {  // alt: the dot pass in the alternative geometry (PencilAlt)
+            if (dot && alt && tb.twp_alt) {
+                using PA = PencilGeom<T, N, ALT>;
+                PS_LTRY(set_smem(k_fwd_x<T, N, true, ALT>, PA::SMEM_DOT));
+                k_fwd_x<T, N, true, ALT><<<blocks, PA::THREADS, PA::SMEM_DOT, st>>>(
+                    data, stride, hvalid, epi, out, ostride, dk, dks, ndk > 0 ? ndk : N, shells, nshell, lut, lut_size,
+                    weight, quad, r2max, partials, tb.twp_alt, mod_out, nc, jband);
+                if (nblocks) *nblocks = (int)blocks;
+                return PS_OK;
+            }
+        }
         if (dot) {
             PS_LTRY(set_smem(k_fwd_x<T, N, true>, PG::SMEM_DOT));
             k_fwd_x<T, N, true><<<blocks, PG::THREADS, PG::SMEM_DOT, st>>>(

@@ -420,6 +420,7 @@ def test_autotuned_plan_and_tune_table(gpu_lib):
     assert table.count("grid ") >= 2, table
     assert "pencil " in table, table  # the Y pass geometry per transform size
     assert "pair " in table, table  # the pair kernel variant per transform size
+    assert "dot " in table, table  # the dot pass geometry per transform size
     scale = np.abs(B64).max()
     assert np.all(np.abs(Bt - B64) <= 1e-5 * np.abs(B64) + 1e-6 * scale)
     np.testing.assert_array_equal(Nt, np.rint(N64))
@@ -440,10 +441,12 @@ def test_autotuned_plan_and_tune_table(gpu_lib):
 
 def test_pair_kernel_variants_from_tune_table(gpu_lib):
     """Every pair kernel variant the autotuner chooses from (0 the default,
-    1 one live row transform, 2 twice the elements per thread), forced through
-    an imported tune table on 128-, 192- and 256-point sub-grids, keeps counts
-    and derived ranges identical and B within the batched tolerance of plain
-    FP64; a table naming a variant outside 0..2 is refused."""
+    1 one live row transform, 2 twice the elements per thread) and both dot
+    pass geometries (1: twice the elements per thread, with pair variants 1
+    and 2), forced through an imported tune table on 128-, 192- and 256-point
+    sub-grids, keep counts and derived ranges identical and B within the
+    batched tolerance of plain FP64; a table naming a variant outside its
+    range is refused."""
     from polyspectrum_b200 import synth
     ps = gpu_lib
     n_grid, box = 256, 400.0
@@ -464,8 +467,9 @@ def test_pair_kernel_variants_from_tune_table(gpu_lib):
         table = "".join(f"grid {g[1]} {g[2]} {g[3]} {g[4]} {max(M, int(g[5]))}\n" for g in grids)
         for v in (0, 1, 2):
             with ps.Context(n_grid, box) as ctx:
-                ctx.tune_import(table + "".join(f"pair {m} {v}\n" for m in (128, 192, 256)))
+                ctx.tune_import(table + "".join(f"pair {m} {v}\ndot {m} {int(v > 0)}\n" for m in (128, 192, 256)))
                 assert f"pair {M} {v}" in ctx.tune_export()
+                assert f"dot {M} {int(v > 0)}" in ctx.tune_export()
                 ctx.get_FT_field(ps.PS_FIELD_XHI_DENS, dens, xhii, use_only_phase=1)
                 plan = ctx.plan(cfgs)
                 Bv, Nv, _, outv = plan.execute()
@@ -479,6 +483,8 @@ def test_pair_kernel_variants_from_tune_table(gpu_lib):
     with ps.Context(n_grid, box) as ctx:
         with pytest.raises(ps.PsError):
             ctx.tune_import("pair 256 3\n")
+        with pytest.raises(ps.PsError):
+            ctx.tune_import("dot 256 2\n")
 
 
 @pytest.mark.parametrize("legs", [(3.1, 4.2, 3.7, 5.0), (4.0, 4.0, 4.0, 4.0), (2.9, 3.6, 4.4, 3.1, 5.2)],
