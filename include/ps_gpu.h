@@ -17,7 +17,8 @@
  *     and are read/written before the call returns.
  *   - One context per host thread; each context runs on its own CUDA stream.
  *   - Grids are N^3, row-major [i][j][l] as in the reference (filter.c:59),
- *     N a power of two in [16, 1024].
+ *     N a power of two in [16, 1024] or one of 48, 60, 96, 192, 300, 320, 384,
+ *     600 (2^a 3^b 5^c; other sizes are refused with PS_ERR_UNSUPPORTED).
  *   - Transforms follow FFTW's unnormalised convention (fft.c:17).
  */
 #ifndef PS_GPU_H
@@ -45,8 +46,9 @@ extern "C" {
  * PS_FP32_BATCHED: all configurations of a call planned together: shells are
  *   deduplicated, shared leg pairs are transformed once, closing legs of a
  *   shared pair are folded by Parseval's identity into one k-space pass, field
- *   transforms run in FP32 with FP64 accumulation, polygon counts are computed
- *   in FP64 and rounded per mode, so they are exact integers. */
+ *   transforms run in FP32 with FP64 accumulation, polygon counts are exact
+ *   integers (counted by enumeration of leg pairs, or by FP64 transforms
+ *   rounded per mode, see PS_PLAN_FFT_COUNTS). */
 #define PS_FP64_PLAIN 1
 #define PS_FP32_BATCHED 2
 
